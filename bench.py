@@ -1,0 +1,352 @@
+"""Benchmark: committed YCSB transactions per second on B200.
+
+Workload (one point of the plain-YCSB scheme sweep): 10,485,760 rows of
+uint64 key + 10 uint64 fields (88 B, stored at a 96 B stride), 1,048,576
+transactions of 16 requests, Zipfian keys (theta), reads with probability
+`read_ratio`, a write stores a fresh uint64 into one uniformly chosen field,
+batch_size 65,536, warp_density 5, block_size 32. A step is one pass of the
+engine over all transactions (metadata reset + ordering passes + transaction
+kernels, gCCTB's tot_time definition, benchmark_cpu/ycsb.cu:249-291).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--scheme tpl_nw]
+  python bench.py --impl reference ...   # the CPU executor on the host cores
+
+Multi-GPU runs are independent replicas (the path does not shard): every
+rank runs the whole workload on its own GPU; value = all ranks' committed
+transactions / max over ranks of the device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+HBM_FALLBACK_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--scheme", default="tpl_nw")
+    ap.add_argument("--theta", type=float, default=0.6)
+    ap.add_argument("--read-ratio", type=float, default=0.9)
+    ap.add_argument("--rows", type=int, default=10_485_760)
+    ap.add_argument("--txs", type=int, default=1_048_576)
+    ap.add_argument("--batch", type=int, default=65_536)
+    ap.add_argument("--wd", type=int, default=5)
+    ap.add_argument("--bs", type=int, default=32)
+    ap.add_argument("--index", default="hash", choices=["hash", "sorted", "direct"])
+    ap.add_argument("--no-reset", action="store_true")
+    ap.add_argument("--cpu-threads", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sweep", default="", help="comma list of extra schemes to time once")
+    return ap.parse_args()
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d.get("hbm_gbs", HBM_FALLBACK_GBS)), "measured"
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+def profile_traffic(scheme):
+    """DRAM bytes per launch of the transaction kernel from a committed ncu
+    summary (profiles/ycsb_kernel_<scheme>.txt, line `traffic_per_launch:`)."""
+    f = ROOT / "profiles" / f"ycsb_kernel_{scheme}.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("traffic_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (clocks + throttle reasons)."""
+
+    def __init__(self, dev):
+        self.dev, self.proc, self.path = dev, None, None
+
+    def start(self):
+        out = ROOT / "gpurun_out"
+        out.mkdir(exist_ok=True)
+        self.path = out / f"clocks_{os.getpid()}.csv"
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def algorithmic_bytes(txs, row_bytes=88, write_bytes=8):
+    """Logical bytes of the committed work (one attempt per tx): the 8 B
+    record header + 8 B per request, and per request a 16 B index probe, a
+    16 B metadata read + update, then the row read (88 B) or the written
+    field (8 B)."""
+    cnt = txs["request_cnt"].astype(np.int64)
+    mask = np.arange(16)[None, :] < cnt[:, None]
+    reads = int((txs["requests"]["read"][mask] != 0).sum())
+    ops = int(cnt.sum())
+    writes = ops - reads
+    return 8 * len(txs) + 8 * ops + reads * (32 + row_bytes) + writes * (32 + write_bytes), reads, writes
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return 0, 1, 0, None
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    rank, local = int(os.environ["RANK"]), int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    return rank, ws, local, dist
+
+
+def reduce_max(dist, v, local):
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(dist, v, local):
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(dist, local):
+    import torch
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(local)
+
+
+def config_of(a):
+    return {
+        "workload": f"ycsb_plain_{a.rows}rows_{a.txs}tx_16ops_theta{a.theta}_r{a.read_ratio}",
+        "cc_scheme": a.scheme, "rows": a.rows, "transactions": a.txs, "ops_per_tx": 16,
+        "theta": a.theta, "read_ratio": a.read_ratio, "batch_size": a.batch,
+        "warp_density": a.wd, "block_size": a.bs, "layout": "u64 key + 10 u64 fields (88 B, 96 B stride)",
+        "write": "fresh uint64 into one uniform field", "index": a.index,
+        "l2": "inputs larger than L2 (1.0 GB table + 143 MB transactions > 126 MB L2)",
+        "parallelism": f"replicas x{a.gpus}",
+    }
+
+
+def cpu_baseline(g, o, txs, a, threads):
+    """The CPU executor (oracle port of the CC rules) on the host cores, on a
+    bounded sample of the same workload."""
+    n = min(len(txs), 262_144)
+    sample = txs[:n]
+    init = o.fill_table(a.rows, 0, 141919810)
+    sch = a.scheme if a.scheme in ("tpl_nw", "silo", "tictoc") else "tpl_nw"
+    t, dg, log, secs, aborts = o.cpu_run(sch, init, 0, sample, g.WRITE_FIELD, 1, threads=threads,
+                                         commit_log=False)
+    nthreads = threads or os.cpu_count()
+    return {"value": n / secs if secs > 0 else 0.0, "unit": "tx/s", "cores": nthreads,
+            "kind": "port", "scheme": sch,
+            "sample": f"first {n} of the {len(txs)} transactions, one pass, {nthreads} threads, "
+                      f"{a.rows} rows"}, secs
+
+
+def run_reference(a):
+    """--impl reference: the CPU port of the path on the host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import gpu_cc_tb_b200 as g
+    from oracle import oracle_py as o
+    txs = g.gen_ycsb(a.rows, a.txs, a.theta, a.read_ratio, seed=141919810,
+                     dedup=g.DEDUP_RESAMPLE, key_base=0)
+    threads = a.cpu_threads or os.cpu_count()
+    sch = a.scheme if a.scheme in ("tpl_nw", "silo", "tictoc") else "tpl_nw"
+    n = min(len(txs), 131_072)
+    init = o.fill_table(a.rows, 0, 141919810)
+    times = []
+    for step in range(a.warmup + a.steps):
+        sample = txs[(step * n) % len(txs):][:n]
+        _, _, _, secs, _ = o.cpu_run(sch, init, 0, sample, g.WRITE_FIELD, 1, threads=threads,
+                                     commit_log=False)
+        if step >= a.warmup:
+            times.append(secs)
+    tot = sum(times)
+    v = a.steps * n / tot
+    cfg = config_of(a)
+    cfg["cc_scheme"] = sch
+    line = {"impl": "reference", "metric": "committed tx/s", "value": v, "unit": "tx/s",
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": 1000 * tot / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded gen_ycsb)",
+            "config": cfg,
+            "cpu_baseline": {"value": v, "unit": "tx/s", "cores": threads, "kind": "port",
+                             "sample": f"{n} transactions per step, {threads} threads"},
+            "e2e": {"value": v, "unit": "tx/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+        return
+    rank, ws, local, dist = dist_init()
+    import torch
+    import gpu_cc_tb_b200 as g
+    index = {"hash": g.INDEX_HASH, "sorted": g.INDEX_SORTED, "direct": g.INDEX_DIRECT}[a.index]
+
+    txs = g.gen_ycsb(a.rows, a.txs, a.theta, a.read_ratio, seed=141919810,
+                     dedup=g.DEDUP_RESAMPLE, key_base=0)
+    alg_bytes, reads, writes = algorithmic_bytes(txs)
+    # pinned host copy of the transactions for the end-to-end leg
+    pinned = torch.empty(txs.nbytes, dtype=torch.uint8, pin_memory=True)
+    host_txs = pinned.numpy().view(g.TX_DTYPE)
+    host_txs[:] = txs
+    digests_host = torch.empty(a.txs * 8, dtype=torch.uint8, pin_memory=True).numpy().view(np.uint64)
+
+    eng = g.Engine(a.rows, layout=g.LAYOUT_U64X11, index=index, fill_seed=141919810,
+                   device=local, max_batch=a.batch)
+    eng.load_txs(host_txs)
+    flags = g.F_NO_RESET if a.no_reset else 0
+    kw = dict(warp_density=a.wd, block_size=a.bs, batch_size=a.batch, flags=flags, write_seed=1)
+    for _ in range(a.warmup):
+        eng.run(a.scheme, **kw)
+
+    clocks = Clocks(local)
+    barrier(dist, local)
+    clocks.start()
+    dev_s, kern_ms, launches, committed, aborts = 0.0, 0.0, 0, 0, 0
+    lat50, lat99 = [], []
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        r = eng.run(a.scheme, **kw)
+        dev_s += r["tot_s"]
+        km, _ = eng.last_kernel_ms()
+        kern_ms += km
+        launches += r["kernel_launches"]
+        committed += r["committed"]
+        aborts += r["aborts"]
+        lat50.append(r["lat_p50_us"])
+        lat99.append(r["lat_p99_us"])
+        n_tx_launches = r["batches"]
+    wall = time.perf_counter() - t0
+    barrier(dist, local)
+    clk = clocks.stop()
+
+    # end to end through the public API: H2D of the step's transactions from
+    # pinned memory, the run, D2H of every transaction's read digest
+    e2e_s = 0.0
+    for _ in range(a.steps):
+        barrier(dist, local)
+        s0 = time.perf_counter()
+        eng.load_txs(host_txs)
+        eng.run(a.scheme, **kw)
+        g.library().gcc_get_digests(eng._h, g.C.c_void_p(digests_host.ctypes.data), a.txs)
+        e2e_s += time.perf_counter() - s0
+
+    dev_s_max = reduce_max(dist, dev_s, local)
+    e2e_max = reduce_max(dist, e2e_s, local)
+    total_committed = reduce_sum(dist, committed, local)
+    value = total_committed / dev_s_max
+    e2e_val = reduce_sum(dist, a.steps * a.txs, local) / e2e_max
+
+    if rank == 0:
+        hbm, kind = peaks()
+        launch_ms = kern_ms / (a.steps * n_tx_launches)
+        per_launch_bytes = alg_bytes / n_tx_launches
+        achieved = per_launch_bytes / (launch_ms / 1000) / 1e9
+        traffic = profile_traffic(a.scheme)
+        line = {
+            "metric": "committed tx/s", "value": value, "unit": "tx/s", "n_gpus": ws,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000 * dev_s_max / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded gen_ycsb, counter-based RNG)",
+            "config": config_of(a),
+            "aborts_per_step": aborts / a.steps,
+            "abort_rate": aborts / max(1, aborts + committed),
+            "latency_us": {"p50": statistics.median(lat50), "p99": statistics.median(lat99)},
+            "wall_s": wall,
+            "e2e": {"value": e2e_val, "unit": "tx/s", "h2d_bytes_per_step": int(txs.nbytes),
+                    "d2h_bytes_per_step": int(a.txs * 8)},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": traffic,
+                         "kernel": "ycsb_kernel", "peak_kind": kind,
+                         "alg_bytes_per_launch": per_launch_bytes,
+                         "launch_ms": launch_ms},
+            "clocks": clk,
+        }
+        if not a.no_cpu_baseline and ws == 1:
+            from oracle import oracle_py as o
+            line["cpu_baseline"], _ = cpu_baseline(g, o, txs, a, a.cpu_threads)
+        if a.sweep:
+            sw = {}
+            for s in a.sweep.split(","):
+                r = eng.run(s, **kw)
+                sw[s] = {"tx_per_s": r["tx_per_s"], "aborts": r["aborts"]}
+            line["sweep"] = sw
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,262 @@
+"""B200 transaction-execution engine for gCCTB's YCSB hot path.
+
+Python mirror of the C ABI in ``include/gcc_engine.h`` (ctypes over the
+in-tree ``lib/libgcctb.so``). It exposes the reference's operator surface:
+the ``cc_scheme`` names, the ``warp_density`` / ``block_size`` /
+``batch_size`` knobs, the gen_ycsb dataset records (136-byte ``YCSBTx``) and
+the 15-column result line of ``test_ycsb`` (gCCTB
+``benchmark_cpu/ycsb.cu:81-302``, ``include/runtime.cuh:169-214``).
+
+There is no CPU execution path: every run goes through the CUDA library, and
+importing fails loudly when it is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+__all__ = [
+    "SCHEMES", "LAYOUT_U64X11", "LAYOUT_REF104", "INDEX_HASH", "INDEX_SORTED",
+    "INDEX_DIRECT", "WRITE_FIELD", "WRITE_ROWCOPY", "F_COMMIT_LOG", "F_READ_LOG",
+    "F_NO_RESET", "DEDUP_DROP", "DEDUP_RESAMPLE", "TX_DTYPE", "GccError", "Engine",
+    "gen_ycsb", "library", "library_path", "scheme_id", "row_bytes", "row_stride",
+]
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libgcctb.so"
+
+# cc_scheme names of test_ycsb (benchmark_cpu/ycsb.cu:168-195)
+SCHEMES = ("tpl_nw", "tpl_wd", "to", "mvcc", "silo", "tictoc", "gacco", "gputx",
+           "slow_tpl_nw", "slow_tpl_wd", "slow_to", "slow_mvcc", "slow_silo", "slow_tictoc")
+
+LAYOUT_U64X11, LAYOUT_REF104 = 0, 1
+INDEX_HASH, INDEX_SORTED, INDEX_DIRECT = 0, 1, 2
+WRITE_FIELD, WRITE_ROWCOPY = 0, 1
+F_COMMIT_LOG, F_READ_LOG, F_NO_RESET = 1, 2, 4
+DEDUP_DROP, DEDUP_RESAMPLE = 0, 1
+
+STATUS = {0: "GCC_OK", -1: "GCC_EINVAL", -2: "GCC_ENOMEM", -3: "GCC_ECUDA", -4: "GCC_ETIMEOUT",
+          -5: "GCC_EFORMAT", -6: "GCC_EKEY", -7: "GCC_EOVERFLOW", -8: "GCC_ESTATE",
+          -9: "GCC_ENODEV"}
+
+# gen_ycsb record: {size_t request_cnt; {int read; unsigned key;}[16]} = 136 B
+TX_DTYPE = np.dtype([("request_cnt", "<u8"),
+                     ("requests", np.dtype([("read", "<i4"), ("key", "<u4")]), (16,))])
+assert TX_DTYPE.itemsize == 136
+
+
+class GccError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        name = STATUS.get(status, str(status))
+        msg = library().gcc_strerror(status).decode()
+        super().__init__(f"{what}: {name} ({msg})" if what else f"{name} ({msg})")
+
+
+class TableDesc(C.Structure):
+    _fields_ = [("rows", C.c_uint64), ("layout", C.c_int32), ("index_kind", C.c_int32),
+                ("fill_seed", C.c_uint64), ("device", C.c_int32), ("max_batch", C.c_int32)]
+
+
+class RunParams(C.Structure):
+    _fields_ = [("cc_scheme", C.c_char_p), ("warp_density", C.c_int32),
+                ("block_size", C.c_int32), ("batch_size", C.c_int32), ("flags", C.c_uint32),
+                ("write_mode", C.c_int32), ("reserved", C.c_int32), ("write_seed", C.c_uint64),
+                ("spin_limit_ns", C.c_uint64)]
+
+
+class Result(C.Structure):
+    _fields_ = [("tx_per_s", C.c_double), ("committed", C.c_uint64), ("aborts", C.c_uint64),
+                ("ts_d", C.c_double), ("wait_d", C.c_double), ("abort_d", C.c_double),
+                ("mng_d", C.c_double), ("tot_d", C.c_double), ("idx_d", C.c_double),
+                ("pre_s", C.c_double), ("proc_s", C.c_double), ("tot_s", C.c_double),
+                ("lat_p50_us", C.c_double), ("lat_p99_us", C.c_double),
+                ("rank_count", C.c_uint64), ("batches", C.c_uint64),
+                ("kernel_launches", C.c_uint64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class CommitRec(C.Structure):
+    _fields_ = [("hi", C.c_uint64), ("lo", C.c_uint64)]
+
+
+_LIB = None
+
+
+def library_path() -> Path:
+    return Path(os.environ.get("GCC_LIB", LIB_PATH))
+
+
+def library() -> C.CDLL:
+    """Load the CUDA C-ABI library (built by gpu_cc_tb_b200/build.py)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = library_path()
+    if not path.exists():
+        raise ImportError(f"{path} is missing: build it with `python gpu_cc_tb_b200/build.py`")
+    lib = C.CDLL(str(path))
+    P = C.c_void_p
+    sig = {
+        "gcc_version": (C.c_char_p, []),
+        "gcc_strerror": (C.c_char_p, [C.c_int]),
+        "gcc_scheme_id": (C.c_int, [C.c_char_p]),
+        "gcc_row_bytes": (C.c_uint32, [C.c_int32]),
+        "gcc_row_stride": (C.c_uint32, [C.c_int32]),
+        "gcc_gen_ycsb": (C.c_int, [C.c_uint64, C.c_uint64, C.c_double, C.c_double, C.c_uint64,
+                                   C.c_int32, C.c_int32, C.c_int32, P]),
+        "gcc_create": (C.c_int, [C.POINTER(TableDesc), C.POINTER(P)]),
+        "gcc_destroy": (None, [P]),
+        "gcc_load_txs": (C.c_int, [P, P, C.c_uint64]),
+        "gcc_run": (C.c_int, [P, C.POINTER(RunParams), C.POINTER(Result)]),
+        "gcc_format_line": (C.c_int, [C.POINTER(RunParams), C.POINTER(Result), C.c_char_p,
+                                      C.c_size_t]),
+        "gcc_dump_table": (C.c_int, [P, P, C.c_uint64]),
+        "gcc_upload_table": (C.c_int, [P, P, C.c_uint64]),
+        "gcc_get_digests": (C.c_int, [P, P, C.c_uint64]),
+        "gcc_get_commit_log": (C.c_int, [P, P, C.c_uint64]),
+        "gcc_get_tx_aborts": (C.c_int, [P, P, C.c_uint64]),
+        "gcc_get_read_log": (C.c_int, [P, P, C.c_uint64]),
+        "gcc_index_lookup": (C.c_int, [P, P, P, C.c_uint64]),
+        "gcc_last_kernel_ms": (C.c_int, [P, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        raise GccError(rc, what)
+
+
+def scheme_id(name: str) -> int:
+    return library().gcc_scheme_id(name.encode())
+
+
+def row_bytes(layout: int) -> int:
+    return library().gcc_row_bytes(layout)
+
+
+def row_stride(layout: int) -> int:
+    return library().gcc_row_stride(layout)
+
+
+def _ptr(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data)
+
+
+def gen_ycsb(rows: int, n_tx: int, theta: float, read_ratio: float, seed: int = 141919810,
+             dedup: int = DEDUP_RESAMPLE, key_base: int = 0, threads: int = 0,
+             out: np.ndarray | None = None) -> np.ndarray:
+    """gen_ycsb dataset as a TX_DTYPE array (generation/gen_ycsb.cu semantics)."""
+    if out is None:
+        out = np.zeros(n_tx, dtype=TX_DTYPE)
+    _check(library().gcc_gen_ycsb(rows, n_tx, theta, read_ratio, seed, dedup, key_base, threads,
+                                  _ptr(out)), "gcc_gen_ycsb")
+    return out
+
+
+class Engine:
+    """One table on one GPU plus its loaded transactions (gcc_engine)."""
+
+    def __init__(self, rows: int, layout: int = LAYOUT_U64X11, index: int = INDEX_HASH,
+                 fill_seed: int = 141919810, device: int = 0, max_batch: int = 65536):
+        self.lib = library()
+        self.rows, self.layout = rows, layout
+        self.row_bytes = row_bytes(layout)
+        self.row_stride = row_stride(layout)
+        self.n_tx = 0
+        d = TableDesc(rows, layout, index, fill_seed, device, max_batch)
+        h = C.c_void_p()
+        _check(self.lib.gcc_create(C.byref(d), C.byref(h)), "gcc_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.gcc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def load_txs(self, txs: np.ndarray):
+        txs = np.ascontiguousarray(txs, dtype=TX_DTYPE)
+        _check(self.lib.gcc_load_txs(self._h, _ptr(txs), len(txs)), "gcc_load_txs")
+        self.n_tx = len(txs)
+
+    def params(self, scheme: str, warp_density: int = 5, block_size: int = 32,
+               batch_size: int = 65536, flags: int = 0, write_mode: int = WRITE_FIELD,
+               write_seed: int = 1, spin_limit_ns: int = 0) -> RunParams:
+        self._scheme = scheme.encode()
+        return RunParams(self._scheme, warp_density, block_size, batch_size, flags, write_mode, 0,
+                         write_seed, spin_limit_ns)
+
+    def run(self, scheme: str, **kw) -> dict:
+        p = self.params(scheme, **kw)
+        r = Result()
+        rc = self.lib.gcc_run(self._h, C.byref(p), C.byref(r))
+        _check(rc, f"gcc_run({scheme})")
+        out = r.as_dict()
+        buf = C.create_string_buffer(512)
+        _check(self.lib.gcc_format_line(C.byref(p), C.byref(r), buf, 512), "gcc_format_line")
+        out["line"] = buf.value.decode()
+        return out
+
+    def dump_table(self) -> np.ndarray:
+        a = np.empty((self.rows, self.row_bytes), dtype=np.uint8)
+        _check(self.lib.gcc_dump_table(self._h, _ptr(a), a.nbytes), "gcc_dump_table")
+        return a
+
+    def upload_table(self, a: np.ndarray):
+        a = np.ascontiguousarray(a, dtype=np.uint8)
+        _check(self.lib.gcc_upload_table(self._h, _ptr(a), a.nbytes), "gcc_upload_table")
+
+    def digests(self) -> np.ndarray:
+        a = np.empty(self.n_tx, dtype=np.uint64)
+        _check(self.lib.gcc_get_digests(self._h, _ptr(a), self.n_tx), "gcc_get_digests")
+        return a
+
+    def tx_aborts(self) -> np.ndarray:
+        a = np.empty(self.n_tx, dtype=np.uint32)
+        _check(self.lib.gcc_get_tx_aborts(self._h, _ptr(a), self.n_tx), "gcc_get_tx_aborts")
+        return a
+
+    def commit_log(self) -> np.ndarray:
+        a = np.empty((self.n_tx, 2), dtype=np.uint64)
+        _check(self.lib.gcc_get_commit_log(self._h, _ptr(a), self.n_tx), "gcc_get_commit_log")
+        return a
+
+    def read_log(self) -> np.ndarray:
+        """Row images read by each (tx, op): shape (n_tx, 16, row_stride) bytes."""
+        a = np.empty((self.n_tx, 16, self.row_stride), dtype=np.uint8)
+        _check(self.lib.gcc_get_read_log(self._h, _ptr(a), a.nbytes), "gcc_get_read_log")
+        return a
+
+    def index_lookup(self, keys) -> np.ndarray:
+        k = np.ascontiguousarray(keys, dtype=np.uint32)
+        r = np.empty_like(k)
+        _check(self.lib.gcc_index_lookup(self._h, _ptr(k), _ptr(r), len(k)), "gcc_index_lookup")
+        return r
+
+    def last_kernel_ms(self):
+        ms, n = C.c_double(), C.c_uint64()
+        _check(self.lib.gcc_last_kernel_ms(self._h, C.byref(ms), C.byref(n)), "gcc_last_kernel_ms")
+        return ms.value, n.value

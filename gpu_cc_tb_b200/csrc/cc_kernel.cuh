@@ -1,0 +1,1115 @@
+// cc_kernel.cuh -- the YCSB transaction kernel under each concurrency-control
+// scheme, written for sm_100a.
+//
+// Reference behaviour followed (gCCTB paths):
+//   transaction loop + retry          benchmark/ycsb.cu:21-111
+//   2PL no-wait / wait-die             include/twopl.cuh:59-382
+//   timestamp ordering                 include/to.cuh:57-271
+//   MVCC                               include/mvcc.cuh:61-297
+//   Silo                               include/silo.cuh:70-339
+//   TicToc                             include/tictoc.cuh:67-369
+//   GaccO ordered hand-off             include/gacco.cuh:49-176
+//   GPUTx rank execution               include/gputx.cuh:58-146
+//   latch ("slow_") variants           include/slow_*.cuh, runtime.cuh:91-109
+//
+// B200 design (not a translation of the reference):
+//   * persistent CTAs; a group of G = 2^warp_density lanes owns one
+//     transaction at a time and takes the next from an ordered ticket;
+//   * the G lanes split the transaction's requests: op i belongs to lane
+//     i % G, so index probes, lock/timestamp operations and row copies of
+//     different requests are in flight together (the reference runs them one
+//     by one on lane 0); group-wide decisions are ballots;
+//   * rows move with 16-byte L2 loads/stores (rows are 16-byte aligned);
+//   * every wait is bounded by `spin_limit_ns` of %globaltimer and raises
+//     GCC_ETIMEOUT instead of hanging.
+//
+// Commit rules are the reference's. Differences that fix reference bugs are
+// listed where they occur (Silo commit timestamp, MVCC base-row update and
+// version-store stride, GPUTx same-rank conflicts).
+#pragma once
+#include <cooperative_groups.h>
+#include "gcc_common.cuh"
+
+namespace gcc {
+
+namespace cg = cooperative_groups;
+
+enum Scheme : int {
+    S_TPL_NW = 0, S_TPL_WD, S_TO, S_MVCC, S_SILO, S_TICTOC, S_GACCO, S_GPUTX,
+    S_SLOW_TPL_NW, S_SLOW_TPL_WD, S_SLOW_TO, S_SLOW_MVCC, S_SLOW_SILO,
+    S_SLOW_TICTOC, S_COUNT
+};
+
+enum AttemptStatus : int { kCommit = 0, kAbort = 1, kGiveUp = 2 };
+
+// Where a bounded wait gave up (Counters::err_where).
+enum WaitSite : unsigned {
+    W_LATCH = 1, W_TPL_WD, W_TO_READ, W_MVCC_READ, W_SILO_READ, W_TICTOC_READ,
+    W_TICTOC_EXT, W_TURN, W_RETRY, W_CAS
+};
+
+// ---------------------------------------------------------------------------
+// A group of G lanes of one warp working on one transaction.
+// ---------------------------------------------------------------------------
+template <int G>
+struct Group {
+    unsigned mask;  // lanes of this group within the warp
+    int base;       // first lane of the group
+    int glane;      // lane within the group
+    GCC_D Group() {
+        int lane = threadIdx.x & 31;
+        base = lane & ~(G - 1);
+        glane = lane & (G - 1);
+        mask = (G == 32) ? 0xFFFFFFFFu : (((1u << G) - 1u) << base);
+    }
+    GCC_D bool any(bool p) const { return __any_sync(mask, p); }
+    GCC_D void sync() const { __syncwarp(mask); }
+    template <class T>
+    GCC_D T bcast(T v, int src) const { return __shfl_sync(mask, v, src, G); }
+    GCC_D unsigned long long sum(unsigned long long v) const {
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, G);
+        return v;
+    }
+    GCC_D unsigned long long maxv(unsigned long long v) const {
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) {
+            unsigned long long u = __shfl_xor_sync(mask, v, o, G);
+            v = u > v ? u : v;
+        }
+        return v;
+    }
+    GCC_D unsigned orv(unsigned v) const {
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) v |= __shfl_xor_sync(mask, v, o, G);
+        return v;
+    }
+};
+
+// Per-transaction lane state: lane owns ops i = glane + k*G, k < K.
+template <int G>
+struct TxOps {
+    static constexpr int K = (kMaxOps + G - 1) / G;
+    uint32_t n;            // requests in the transaction
+    uint32_t valid;        // bit k: op k exists
+    uint32_t isread;       // bit k: op k reads
+    uint32_t readmask;     // group-wide: bit i set if op i reads
+    uint32_t row[K];
+};
+
+// Bounded wait helper: true once `limit` ns have passed since `t0`.
+GCC_D bool expired(uint64_t t0, uint64_t limit) { return gtimer() - t0 > limit; }
+
+// ---------------------------------------------------------------------------
+// Row images: digest, read log, rowcopy scratch, writes.
+// ---------------------------------------------------------------------------
+constexpr int kMaxChunks = 7;  // 16-byte chunks cover up to 14 words (112 B)
+
+GCC_D size_t slot_of(const KParams &p, uint64_t unit, uint32_t i) {
+    return ((size_t)unit * kMaxOps + i) * p.wslot;
+}
+// Stream a row image from `src` (16-byte L2 loads), folding its words into
+// the digest term `dt` of op i and copying it to the rowcopy scratch slot and
+// the read log when those exist. Nothing is held in registers beyond one
+// chunk, so the transaction kernel fits 64 registers.
+GCC_D void read_image(const KParams &p, const uint64_t *src, uint32_t tx, uint64_t pos,
+                      uint32_t i, unsigned long long &dt) {
+    const ulonglong2 *s = (const ulonglong2 *)src;
+    ulonglong2 *sc = p.scratch ? (ulonglong2 *)(p.scratch + slot_of(p, pos, i)) : nullptr;
+    ulonglong2 *lg = p.read_log ? (ulonglong2 *)(p.read_log + slot_of(p, tx, i)) : nullptr;
+#pragma unroll
+    for (int c = 0; c < kMaxChunks; ++c) {
+        if (2 * c < (int)p.words) {
+            ulonglong2 v = __ldcg(s + c);
+            dt += digest_term(v.x, i, 2u * c);
+            if (2 * c + 1 < (int)p.words) dt += digest_term(v.y, i, 2u * c + 1u);
+            if (sc) __stcg(sc + c, v);
+            if (lg) __stcg(lg + c, v);
+        }
+    }
+}
+GCC_D void copy_image(const KParams &p, uint64_t *dst, const uint64_t *src) {
+#pragma unroll
+    for (int c = 0; c < kMaxChunks; ++c)
+        if (2 * c < (int)p.words)
+            __stcg((ulonglong2 *)dst + c, __ldcg((const ulonglong2 *)src + c));
+}
+// Last read op before op i (program order), -1 if none.
+GCC_D int rowcopy_src(uint32_t readmask, uint32_t i) {
+    uint32_t m = readmask & ((1u << i) - 1u);
+    return m ? 31 - __clz(m) : -1;
+}
+// Apply write op i of tx to `row` (GCC_WRITE_FIELD or GCC_WRITE_ROWCOPY).
+GCC_D void apply_write(const KParams &p, uint32_t row, uint32_t tx, uint64_t pos,
+                       uint32_t i, uint32_t readmask) {
+    uint64_t *r = row_ptr(p, row);
+    if (p.write_mode == GCC_WRITE_FIELD) {
+        uint32_t f = write_field(p.write_seed, tx, i);
+        __stcg((unsigned long long *)(r + 1 + f),
+               (unsigned long long)write_value(p.write_seed, tx, i));
+        return;
+    }
+    int src = rowcopy_src(readmask, i);
+    if (src < 0) {
+#pragma unroll
+        for (int c = 0; c < kMaxChunks; ++c)
+            if (2 * c < (int)p.words) __stcg((ulonglong2 *)r + c, make_ulonglong2(0ull, 0ull));
+    } else {
+        copy_image(p, r, p.scratch + slot_of(p, pos, (uint32_t)src));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Latches of the slow_* variants (runtime.cuh:91-109), bounded.
+// ---------------------------------------------------------------------------
+GCC_D bool latch_acquire(const KParams &p, uint32_t row) {
+    unsigned *l = p.latch + row;
+    if (atomicCAS(l, 0u, 1u) == 0u) { __threadfence(); return true; }
+    uint64_t t0 = gtimer();
+    while (true) {
+        if (atomicCAS(l, 0u, 1u) == 0u) { __threadfence(); return true; }
+        if (expired(t0, p.spin_limit_ns) || error_raised(p.ctr)) {
+            set_error(p.ctr, GCC_ETIMEOUT, W_LATCH);
+            return false;
+        }
+    }
+}
+GCC_D void latch_release(const KParams &p, uint32_t row) {
+    __threadfence();
+    atomicExch(p.latch + row, 0u);
+}
+
+// Warp-aggregated timestamp allocation among the group leaders that arrive
+// together (one atomic per warp instead of one per transaction).
+GCC_D unsigned long long alloc_ts(Counters *c) {
+    cg::coalesced_group act = cg::coalesced_threads();
+    unsigned long long base = 0;
+    if (act.thread_rank() == 0) base = atomicAdd(&c->ts, (unsigned long long)act.size());
+    base = act.shfl(base, 0);
+    return base + act.thread_rank();
+}
+
+// Per-attempt leader-side timing accumulators.
+struct Clocks {
+    unsigned long long ts, wait, mng;
+};
+
+// ===========================================================================
+// 2PL no-wait / wait-die (twopl.cuh:233-322; slow_twopl.cuh:238-331)
+// ===========================================================================
+enum LockResult : int { L_OK = 0, L_DIE = 1, L_WAIT = 2, L_ERR = 3 };
+
+template <bool WD>
+GCC_D int tpl_shared(const KParams &p, uint32_t row, uint32_t tx) {
+    unsigned long long *m = p.meta + row;
+    if (WD) {
+        unsigned long long w = ld_cg(m);
+        if (w & tpl::kExcl) return tpl::holder(w) < tx ? L_DIE : L_WAIT;
+    }
+    unsigned long long old = atomicAdd(m, 1ull);
+    if (!(old & tpl::kExcl)) return L_OK;
+    atomicAdd(m, ~0ull);  // undo the speculative reader increment
+    if (!WD) return L_DIE;
+    return tpl::holder(old) < tx ? L_DIE : L_WAIT;
+}
+template <bool WD>
+GCC_D int tpl_excl(const KParams &p, uint32_t row, uint32_t tx) {
+    unsigned long long old = atomicCAS(p.meta + row, 0ull, tpl::excl_word(tx));
+    if (old == 0ull) return L_OK;
+    if (!WD) return L_DIE;
+    if (!(old & tpl::kExcl)) return L_DIE;  // shared holders: requester dies
+    return tpl::holder(old) < tx ? L_DIE : L_WAIT;
+}
+// Latch variants: plain read/modify/write of the same word under a latch.
+template <bool WD>
+GCC_D int slow_tpl_lock(const KParams &p, uint32_t row, uint32_t tx, bool shared) {
+    if (!latch_acquire(p, row)) return L_ERR;
+    volatile unsigned long long *m = p.meta + row;
+    unsigned long long w = *m;
+    int r;
+    if (shared) {
+        if (!(w & tpl::kExcl)) { *m = w + 1ull; r = L_OK; }
+        else r = (!WD || tpl::holder(w) < tx) ? L_DIE : L_WAIT;
+    } else {
+        if (w == 0ull) { *m = tpl::excl_word(tx); r = L_OK; }
+        else if (!WD || !(w & tpl::kExcl)) r = L_DIE;
+        else r = tpl::holder(w) < tx ? L_DIE : L_WAIT;
+    }
+    latch_release(p, row);
+    return r;
+}
+template <bool SLOW>
+GCC_D bool tpl_unlock(const KParams &p, uint32_t row, bool shared) {
+    if (!SLOW) {
+        if (shared) atomicAdd(p.meta + row, ~0ull);
+        else atomicAnd(p.meta + row, tpl::kReaders);
+        return true;
+    }
+    if (shared) {
+        if (!latch_acquire(p, row)) return false;
+        volatile unsigned long long *m = p.meta + row;
+        *m = *m - 1ull;
+        latch_release(p, row);
+    } else {
+        // the exclusive holder is the only writer of the word
+        // (slow_twopl.cuh:333-338 stores without the latch)
+        __threadfence();
+        atomicExch(p.meta + row, 0ull);
+    }
+    return true;
+}
+
+template <bool WD, bool SLOW>
+GCC_D int tpl_lock(const KParams &p, uint32_t row, uint32_t tx, bool rd) {
+    return SLOW ? slow_tpl_lock<WD>(p, row, tx, rd)
+                : (rd ? tpl_shared<WD>(p, row, tx) : tpl_excl<WD>(p, row, tx));
+}
+
+// First attempts take all locks at once (one ballot decides); retries take
+// them one request at a time in request (= ascending key) order, as the
+// reference does, so that competing transactions cannot keep aborting each
+// other. Both apply the scheme's rule: a conflict means abort (no-wait) or
+// wait-or-die by transaction age (wait-die).
+template <int G, bool WD, bool SLOW>
+GCC_D int attempt_tpl(const KParams &p, const Group<G> &g, const TxOps<G> &s, uint32_t tx,
+                      uint64_t pos, unsigned long long &dg, Clocks &ck, bool ordered) {
+    constexpr int K = TxOps<G>::K;
+    uint32_t held = 0, pending = s.valid;
+    bool fail = false, err = false;
+    uint64_t t0 = gtimer();
+    long long cw = clock64();
+    bool first = true;
+    if (ordered) {
+        for (uint32_t i = 0; i < s.n && !fail; ++i) {
+            const int owner = (int)(i % G), kk = (int)(i / G);
+            int r = L_OK;
+            if (g.glane == owner) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    if (k != kk) continue;
+                    while (true) {
+                        r = tpl_lock<WD, SLOW>(p, s.row[k], tx, (s.isread >> k) & 1u);
+                        if (r != L_WAIT) break;
+                        if (first) { first = false; cw = clock64(); }
+                        if (expired(t0, p.spin_limit_ns) || error_raised(p.ctr)) {
+                            set_error(p.ctr, GCC_ETIMEOUT, W_TPL_WD);
+                            r = L_ERR;
+                            break;
+                        }
+                    }
+                    if (r == L_OK) held |= 1u << k;
+                }
+            }
+            r = g.bcast(r, owner);
+            if (r == L_DIE) fail = true;
+            else if (r == L_ERR) { fail = true; err = true; }
+        }
+    } else {
+        while (true) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                if (!((pending >> k) & 1u) || fail || err) continue;
+                int r = tpl_lock<WD, SLOW>(p, s.row[k], tx, (s.isread >> k) & 1u);
+                if (r == L_OK) { held |= 1u << k; pending &= ~(1u << k); }
+                else if (r == L_DIE) fail = true;
+                else if (r == L_ERR) err = true;
+            }
+            bool gf = g.any(fail), ge = g.any(err), gp = g.any(pending != 0u);
+            if (ge) { fail = true; err = true; break; }
+            if (gf || !gp) { fail = gf; break; }
+            if (first) { first = false; cw = clock64(); }
+            if (g.any(expired(t0, p.spin_limit_ns) || error_raised(p.ctr))) {
+                if (g.glane == 0) set_error(p.ctr, GCC_ETIMEOUT, W_TPL_WD);
+                fail = true; err = true; break;
+            }
+        }
+    }
+    if (!first) ck.wait += clock64() - cw;
+    if (fail) {
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            if ((held >> k) & 1u) tpl_unlock<SLOW>(p, s.row[k], (s.isread >> k) & 1u);
+        return err ? kGiveUp : kAbort;
+    }
+    __threadfence();
+    // Serialization point: every lock is held.
+    if ((p.flags & GCC_F_COMMIT_LOG) && g.glane == 0) {
+        p.commit_hi[tx] = atomicAdd(&p.ctr->seq, 1ull);
+        p.commit_lo[tx] = 0ull;
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        if (((s.valid & s.isread) >> k) & 1u) {
+            read_image(p, row_ptr(p, s.row[k]), tx, pos, (uint32_t)(g.glane + k * G), dg);
+        }
+    }
+    if (p.write_mode == GCC_WRITE_ROWCOPY) g.sync();
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        if (((s.valid & ~s.isread) >> k) & 1u)
+            apply_write(p, s.row[k], tx, pos, (uint32_t)(g.glane + k * G), s.readmask);
+    __threadfence();
+    bool uerr = false;
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        if ((s.valid >> k) & 1u) uerr |= !tpl_unlock<SLOW>(p, s.row[k], (s.isread >> k) & 1u);
+    return g.any(uerr) ? kGiveUp : kCommit;
+}
+
+// ===========================================================================
+// Timestamp ordering (to.cuh:104-270; slow_to.cuh:137-238)
+// ===========================================================================
+enum OpResult : int { O_DONE = 0, O_FAIL = 1, O_RETRY = 2, O_ERR = 3 };
+
+template <bool SLOW>
+GCC_D int to_read(const KParams &p, uint32_t row, uint64_t ts, uint32_t tx, uint64_t pos,
+                  uint32_t i, unsigned long long &dt) {
+    unsigned long long *m = p.meta + row;
+    if (SLOW) {
+        if (!latch_acquire(p, row)) return O_ERR;
+        unsigned long long x = *(volatile unsigned long long *)m;
+        int r;
+        if (tso::wts(x) > ts) r = O_FAIL;
+        else if (x & tso::kUnc) r = O_RETRY;
+        else {
+            read_image(p, row_ptr(p, row), tx, pos, i, dt);
+            uint64_t rts = tso::rts(x) > ts ? tso::rts(x) : ts;
+            *(volatile unsigned long long *)m = tso::make(false, rts, tso::wts(x));
+            r = O_DONE;
+        }
+        latch_release(p, row);
+        return r;
+    }
+    unsigned long long x = ld_cg(m);
+    if (tso::wts(x) > ts) return O_FAIL;
+    if (x & tso::kUnc) return O_RETRY;  // wait for the older writer
+    read_image(p, row_ptr(p, row), tx, pos, i, dt);
+    if (tso::rts(x) >= ts) {
+        // rts already covers this reader: only check the snapshot held
+        __threadfence();
+        return ld_cg(m) == x ? O_DONE : O_RETRY;
+    }
+    unsigned long long nx = tso::make(false, ts, tso::wts(x));
+    return atomicCAS(m, x, nx) == x ? O_DONE : O_RETRY;
+}
+template <bool SLOW>
+GCC_D int to_write(const KParams &p, uint32_t row, uint64_t ts, unsigned long long &prev) {
+    unsigned long long *m = p.meta + row;
+    if (SLOW) {
+        if (!latch_acquire(p, row)) return O_ERR;
+        unsigned long long x = *(volatile unsigned long long *)m;
+        int r;
+        if (tso::rts(x) > ts || tso::wts(x) > ts || (x & tso::kUnc)) r = O_FAIL;
+        else { prev = x; *(volatile unsigned long long *)m = tso::make(true, ts, ts); r = O_DONE; }
+        latch_release(p, row);
+        return r;
+    }
+    unsigned long long x = ld_cg(m);
+    if (tso::rts(x) > ts || tso::wts(x) > ts || (x & tso::kUnc)) return O_FAIL;
+    if (atomicCAS(m, x, tso::make(true, ts, ts)) != x) return O_RETRY;
+    prev = x;
+    return O_DONE;
+}
+
+template <int G, bool SLOW>
+GCC_D int attempt_to(const KParams &p, const Group<G> &g, const TxOps<G> &s, uint32_t tx,
+                     uint64_t pos, unsigned long long &dg, Clocks &ck, bool ordered) {
+    constexpr int K = TxOps<G>::K;
+    unsigned long long ts = 0;
+    if (g.glane == 0) {
+        long long c0 = clock64();
+        ts = alloc_ts(p.ctr);
+        ck.ts += clock64() - c0;
+    }
+    ts = g.bcast(ts, 0);
+    if (ts > tso::kTsMax) {
+        if (g.glane == 0) set_error(p.ctr, GCC_EOVERFLOW, 0);
+        return kGiveUp;
+    }
+    uint32_t pending = s.valid, wrote = 0;
+    unsigned long long prev[K];
+    bool fail = false, err = false;
+    uint64_t t0 = gtimer();
+    bool first = true;
+    long long cw = 0;
+    while (true) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (!((pending >> k) & 1u) || fail || err) continue;
+            uint32_t i = g.glane + k * G;
+            int r;
+            if ((s.isread >> k) & 1u) {
+                unsigned long long dt = 0;
+                r = to_read<SLOW>(p, s.row[k], ts, tx, pos, i, dt);
+                if (r == O_DONE) dg += dt;
+            } else {
+                r = to_write<SLOW>(p, s.row[k], ts, prev[k]);
+                if (r == O_DONE) wrote |= 1u << k;
+            }
+            if (r == O_DONE) pending &= ~(1u << k);
+            else if (r == O_FAIL) fail = true;
+            else if (r == O_ERR) err = true;
+        }
+        bool ge = g.any(err), gf = g.any(fail), gp = g.any(pending != 0u);
+        if (ge) { fail = err = true; break; }
+        if (gf || !gp) { fail = gf; break; }
+        if (first) { first = false; cw = clock64(); }
+        if (g.any(expired(t0, p.spin_limit_ns) || error_raised(p.ctr))) {
+            if (g.glane == 0) set_error(p.ctr, GCC_ETIMEOUT, W_TO_READ);
+            fail = err = true; break;
+        }
+    }
+    if (!first) ck.wait += clock64() - cw;
+    if (fail) {
+        // restore the words this attempt marked uncommitted (to.cuh:255-270)
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            if ((wrote >> k) & 1u) atomicExch(p.meta + s.row[k], prev[k]);
+        __threadfence();
+        return err ? kGiveUp : kAbort;
+    }
+    // Serialization key: (batch, timestamp); timestamps restart per batch.
+    if ((p.flags & GCC_F_COMMIT_LOG) && g.glane == 0) {
+        p.commit_hi[tx] = p.batch_st;
+        p.commit_lo[tx] = ts;
+    }
+    if (p.write_mode == GCC_WRITE_ROWCOPY) g.sync();
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        if ((wrote >> k) & 1u) apply_write(p, s.row[k], tx, pos, g.glane + k * G, s.readmask);
+    __threadfence();
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        if ((wrote >> k) & 1u) atomicExch(p.meta + s.row[k], tso::make(false, ts, ts));
+    return kCommit;
+}
+
+// ===========================================================================
+// MVCC (mvcc.cuh:113-297). Requests run one at a time in program order (the
+// reader waits on any uncommitted version, as in the reference, and
+// ascending-key access keeps those waits acyclic). Two reference defects are
+// not reproduced: the base row is updated at commit (mvcc.cuh:143 leaves the
+// copy commented out) and each version owns a full row image (mvcc.cuh:142
+// strides the version data by sizeof(version_node)).
+// ===========================================================================
+template <bool SLOW>
+GCC_D int mvcc_read(const KParams &p, uint32_t row, uint64_t ts, uint32_t tx, uint64_t pos,
+                    uint32_t i, unsigned long long &dt) {
+    unsigned long long *m = p.meta + row;
+    if (SLOW && !latch_acquire(p, row)) return O_ERR;
+    unsigned long long x = SLOW ? *(volatile unsigned long long *)m : ld_cg(m);
+    int r;
+    if (x & tso::kUnc) {
+        r = O_RETRY;
+    } else if (tso::wts(x) <= ts) {
+        read_image(p, row_ptr(p, row), tx, pos, i, dt);
+        if (tso::rts(x) >= ts) {
+            __threadfence();
+            r = (SLOW || ld_cg(m) == x) ? O_DONE : O_RETRY;
+        } else if (SLOW) {
+            *(volatile unsigned long long *)m = tso::make(false, ts, tso::wts(x));
+            r = O_DONE;
+        } else {
+            r = atomicCAS(m, x, tso::make(false, ts, tso::wts(x))) == x ? O_DONE : O_RETRY;
+        }
+    } else {
+        // walk the version chain to the newest version with wts <= ts
+        unsigned node = ld_cg(p.turn + row);
+        unsigned hops = 0;
+        while (node != kNoRow && tso::wts(ld_cg(p.ver_ts + node)) > ts && hops < 0x1000000u) {
+            node = ld_cg(p.ver_prev + node);
+            ++hops;
+        }
+        if (node == kNoRow || hops >= 0x1000000u) {
+            set_error(p.ctr, GCC_EFORMAT, W_MVCC_READ);  // broken chain
+            r = O_ERR;
+        } else {
+            read_image(p, p.ver_data + (size_t)node * p.wslot, tx, pos, i, dt);
+            __threadfence();
+            r = (SLOW || ld_cg(m) == x) ? O_DONE : O_RETRY;
+        }
+    }
+    if (SLOW) latch_release(p, row);
+    return r;
+}
+
+template <int G, bool SLOW>
+GCC_D int attempt_mvcc(const KParams &p, const Group<G> &g, const TxOps<G> &s, uint32_t tx,
+                       uint64_t pos, unsigned long long &dg, Clocks &ck, bool ordered) {
+    constexpr int K = TxOps<G>::K;
+    unsigned long long ts = 0;
+    if (g.glane == 0) {
+        long long c0 = clock64();
+        ts = alloc_ts(p.ctr);
+        ck.ts += clock64() - c0;
+    }
+    ts = g.bcast(ts, 0);
+    if (ts > tso::kTsMax) {
+        if (g.glane == 0) set_error(p.ctr, GCC_EOVERFLOW, 0);
+        return kGiveUp;
+    }
+    uint32_t wrote = 0;
+    unsigned long long prev[K];
+    bool fail = false, err = false;
+    for (uint32_t i = 0; i < s.n; ++i) {
+        const int owner = (int)(i % G);
+        const int kk = (int)(i / G);
+        if (g.glane == owner) {
+            uint64_t t0 = gtimer();
+            long long cw = clock64();
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                if (k != kk) continue;
+                while (true) {
+                    int r;
+                    if ((s.isread >> k) & 1u) {
+                        unsigned long long dt = 0;
+                        r = mvcc_read<SLOW>(p, s.row[k], ts, tx, pos, i, dt);
+                        if (r == O_DONE) dg += dt;
+                    } else {
+                        r = to_write<SLOW>(p, s.row[k], ts, prev[k]);
+                        if (r == O_DONE) wrote |= 1u << k;
+                    }
+                    if (r == O_DONE) break;
+                    if (r == O_FAIL) { fail = true; break; }
+                    if (r == O_ERR) { err = true; break; }
+                    if (expired(t0, p.spin_limit_ns) || error_raised(p.ctr)) {
+                        set_error(p.ctr, GCC_ETIMEOUT, W_MVCC_READ);
+                        err = true;
+                        break;
+                    }
+                }
+            }
+            ck.wait += clock64() - cw;
+        }
+        bool gf = g.any(fail), ge = g.any(err);
+        if (gf || ge) { fail = true; err = ge; break; }
+    }
+    if (fail) {
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            if ((wrote >> k) & 1u) atomicExch(p.meta + s.row[k], prev[k]);
+        __threadfence();
+        return err ? kGiveUp : kAbort;
+    }
+    // Serialization key: (batch, timestamp); timestamps restart per batch.
+    if ((p.flags & GCC_F_COMMIT_LOG) && g.glane == 0) {
+        p.commit_hi[tx] = p.batch_st;
+        p.commit_lo[tx] = ts;
+    }
+    if (p.write_mode == GCC_WRITE_ROWCOPY) g.sync();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        if (!((wrote >> k) & 1u)) continue;
+        uint32_t i = g.glane + k * G;
+        uint32_t row = s.row[k];
+        // push the current base row as the version it replaces, link it,
+        // then install the new base row and publish (uncommitted -> 0)
+        uint32_t node = (uint32_t)(pos * kMaxOps + i);
+        copy_image(p, p.ver_data + (size_t)node * p.wslot, row_ptr(p, row));
+        p.ver_ts[node] = prev[k];
+        p.ver_prev[node] = ld_cg(p.turn + row);
+        __threadfence();
+        atomicExch(p.turn + row, node);
+        apply_write(p, row, tx, pos, i, s.readmask);
+        __threadfence();
+        atomicExch(p.meta + row, tso::make(false, ts, ts));
+    }
+    return kCommit;
+}
+
+// ===========================================================================
+// Silo (silo.cuh:116-338; slow_silo.cuh:188-326). The commit timestamp is
+// max(read-set ts, current write-set ts) + 1 as in Silo; the reference takes
+// the write-set term from a field Write never sets (silo.cuh:306-310), which
+// lets a record's ts repeat and a stale read validate.
+// ===========================================================================
+template <bool SLOW>
+GCC_D int silo_read(const KParams &p, uint32_t row, uint32_t tx, uint64_t pos, uint32_t i,
+                    unsigned long long &dt, unsigned long long &ts) {
+    unsigned long long *m = p.meta + row;
+    if (SLOW) {
+        if (!latch_acquire(p, row)) return O_ERR;
+        unsigned long long x = *(volatile unsigned long long *)m;
+        int r = O_RETRY;
+        if (!(x & silo::kLock)) { read_image(p, row_ptr(p, row), tx, pos, i, dt); ts = silo::ts(x); r = O_DONE; }
+        latch_release(p, row);
+        return r;
+    }
+    unsigned long long x1 = ld_cg(m);
+    if (x1 & silo::kLock) return O_RETRY;
+    __threadfence();
+    read_image(p, row_ptr(p, row), tx, pos, i, dt);
+    __threadfence();
+    unsigned long long x2 = ld_cg(m);
+    if (x1 != x2) return O_RETRY;
+    ts = silo::ts(x1);
+    return O_DONE;
+}
+// No-wait write lock: O_DONE (cur = word before locking), O_FAIL if locked.
+template <bool SLOW>
+GCC_D int occ_lock(const KParams &p, uint32_t row, unsigned long long lockbit,
+                   unsigned long long &cur) {
+    unsigned long long *m = p.meta + row;
+    if (SLOW) {
+        if (!latch_acquire(p, row)) return O_ERR;
+        unsigned long long x = *(volatile unsigned long long *)m;
+        int r = O_FAIL;
+        if (!(x & lockbit)) { *(volatile unsigned long long *)m = x | lockbit; cur = x; r = O_DONE; }
+        latch_release(p, row);
+        return r;
+    }
+    for (int tries = 0; tries < 1 << 20; ++tries) {
+        unsigned long long x = ld_cg(m);
+        if (x & lockbit) return O_FAIL;
+        if (atomicCAS(m, x, x | lockbit) == x) { cur = x; return O_DONE; }
+    }
+    set_error(p.ctr, GCC_ETIMEOUT, W_CAS);
+    return O_ERR;
+}
+
+// Lock the write set, no-wait (silo.cuh:268-281, tictoc.cuh:269-282). First
+// attempts lock in parallel; retries lock one request at a time in request
+// order. `cts` accumulates f(word before locking) over the locked words.
+template <int G, bool SLOW, bool TICTOC>
+GCC_D void occ_lock_writes(const KParams &p, const Group<G> &g, const TxOps<G> &s,
+                           uint32_t writes, bool ordered, uint32_t &held,
+                           unsigned long long &cts, bool &fail, bool &err) {
+    constexpr int K = TxOps<G>::K;
+    const unsigned long long lockbit = TICTOC ? tictoc::kLock : silo::kLock;
+    if (!ordered) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (!((writes >> k) & 1u) || fail || err) continue;
+            unsigned long long cur;
+            int r = occ_lock<SLOW>(p, s.row[k], lockbit, cur);
+            if (r == O_DONE) {
+                held |= 1u << k;
+                unsigned long long c = TICTOC ? tictoc::rts(cur) + 1ull : silo::ts(cur);
+                cts = cts > c ? cts : c;
+            } else if (r == O_FAIL) fail = true;
+            else err = true;
+        }
+        return;
+    }
+    for (uint32_t i = 0; i < s.n; ++i) {
+        const int owner = (int)(i % G), kk = (int)(i / G);
+        int r = O_DONE;
+        if (g.glane == owner) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                if (k != kk || !((writes >> k) & 1u)) continue;
+                unsigned long long cur;
+                r = occ_lock<SLOW>(p, s.row[k], lockbit, cur);
+                if (r == O_DONE) {
+                    held |= 1u << k;
+                    unsigned long long c = TICTOC ? tictoc::rts(cur) + 1ull : silo::ts(cur);
+                    cts = cts > c ? cts : c;
+                }
+            }
+        }
+        r = g.bcast(r, owner);
+        if (r == O_FAIL) { fail = true; break; }
+        if (r == O_ERR) { err = true; break; }
+    }
+}
+
+template <int G, bool SLOW>
+GCC_D int attempt_silo(const KParams &p, const Group<G> &g, const TxOps<G> &s, uint32_t tx,
+                       uint64_t pos, unsigned long long &dg, Clocks &ck, bool ordered) {
+    constexpr int K = TxOps<G>::K;
+    unsigned long long rec[K];
+    uint32_t reads = s.valid & s.isread, writes = s.valid & ~s.isread;
+    uint32_t pending = reads, held = 0;
+    bool fail = false, err = false;
+    // read phase: consistent snapshots (silo.cuh:223-259)
+    uint64_t t0 = gtimer();
+    bool first = true;
+    long long cw = 0;
+    while (true) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (!((pending >> k) & 1u) || err) continue;
+            unsigned long long dt = 0;
+            int r = silo_read<SLOW>(p, s.row[k], tx, pos, g.glane + k * G, dt, rec[k]);
+            if (r == O_DONE) { pending &= ~(1u << k); dg += dt; }
+            else if (r == O_ERR) err = true;
+        }
+        bool ge = g.any(err), gp = g.any(pending != 0u);
+        if (ge) return kGiveUp;
+        if (!gp) break;
+        if (first) { first = false; cw = clock64(); }
+        if (g.any(expired(t0, p.spin_limit_ns) || error_raised(p.ctr))) {
+            if (g.glane == 0) set_error(p.ctr, GCC_ETIMEOUT, W_SILO_READ);
+            return kGiveUp;
+        }
+    }
+    if (!first) ck.wait += clock64() - cw;
+    // validation: lock the write set, no-wait (silo.cuh:268-281)
+    unsigned long long cts = 0;
+    occ_lock_writes<G, SLOW, false>(p, g, s, writes, ordered, held, cts, fail, err);
+    bool gf = g.any(fail), ge = g.any(err);
+    if (!gf && !ge) {
+        __threadfence();
+        // Serialization point: write set locked, read set not yet validated.
+        if ((p.flags & GCC_F_COMMIT_LOG) && g.glane == 0) {
+            p.commit_hi[tx] = atomicAdd(&p.ctr->seq, 1ull);
+            p.commit_lo[tx] = 0ull;
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (!((reads >> k) & 1u)) continue;
+            unsigned long long x = ld_cg(p.meta + s.row[k]);
+            if (silo::ts(x) != rec[k] || (x & silo::kLock)) fail = true;
+            cts = cts > rec[k] ? cts : rec[k];
+        }
+        gf = g.any(fail);
+    }
+    if (gf || ge) {
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            if ((held >> k) & 1u) atomicAnd(p.meta + s.row[k], ~silo::kLock);
+        __threadfence();
+        return ge ? kGiveUp : kAbort;
+    }
+    cts = g.maxv(cts) + 1ull;
+    if (p.write_mode == GCC_WRITE_ROWCOPY) g.sync();
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        if ((writes >> k) & 1u) apply_write(p, s.row[k], tx, pos, g.glane + k * G, s.readmask);
+    __threadfence();
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        if ((writes >> k) & 1u) atomicExch(p.meta + s.row[k], cts);
+    return kCommit;
+}
+
+// ===========================================================================
+// TicToc (tictoc.cuh:115-368; slow_tictoc.cuh)
+// ===========================================================================
+template <bool SLOW>
+GCC_D int tictoc_read(const KParams &p, uint32_t row, uint32_t tx, uint64_t pos, uint32_t i,
+                      unsigned long long &dt, unsigned long long &wts, unsigned long long &rts) {
+    unsigned long long *m = p.meta + row;
+    if (SLOW) {
+        if (!latch_acquire(p, row)) return O_ERR;
+        unsigned long long x = *(volatile unsigned long long *)m;
+        int r = O_RETRY;
+        if (!(x & tictoc::kLock)) {
+            read_image(p, row_ptr(p, row), tx, pos, i, dt);
+            wts = tictoc::wts(x); rts = tictoc::rts(x); r = O_DONE;
+        }
+        latch_release(p, row);
+        return r;
+    }
+    unsigned long long x1 = ld_cg(m);
+    if (x1 & tictoc::kLock) return O_RETRY;
+    __threadfence();
+    read_image(p, row_ptr(p, row), tx, pos, i, dt);
+    __threadfence();
+    if (ld_cg(m) != x1) return O_RETRY;
+    wts = tictoc::wts(x1);
+    rts = tictoc::rts(x1);
+    return O_DONE;
+}
+// Extend a read version's rts to cover commit_ts (tictoc.cuh:302-340).
+template <bool SLOW>
+GCC_D int tictoc_extend(const KParams &p, uint32_t row, unsigned long long rwts,
+                        unsigned long long cts) {
+    unsigned long long *m = p.meta + row;
+    for (int tries = 0; tries < 1 << 20; ++tries) {
+        if (SLOW && !latch_acquire(p, row)) return O_ERR;
+        unsigned long long x = SLOW ? *(volatile unsigned long long *)m : ld_cg(m);
+        unsigned long long wts = tictoc::wts(x), rts = tictoc::rts(x);
+        int r;
+        if (wts != rwts || (rts <= cts && (x & tictoc::kLock))) {
+            r = O_FAIL;
+        } else if (rts > cts) {
+            r = O_DONE;
+        } else {
+            unsigned long long delta = cts - wts;
+            unsigned long long shift = delta - (delta & 0x7FFFull);
+            unsigned long long nx = tictoc::make(false, delta - shift, wts + shift);
+            if (SLOW) { *(volatile unsigned long long *)m = nx; r = O_DONE; }
+            else r = atomicCAS(m, x, nx) == x ? O_DONE : O_RETRY;
+        }
+        if (SLOW) latch_release(p, row);
+        if (r != O_RETRY) return r;
+    }
+    set_error(p.ctr, GCC_ETIMEOUT, W_TICTOC_EXT);
+    return O_ERR;
+}
+
+template <int G, bool SLOW>
+GCC_D int attempt_tictoc(const KParams &p, const Group<G> &g, const TxOps<G> &s, uint32_t tx,
+                         uint64_t pos, unsigned long long &dg, Clocks &ck, bool ordered) {
+    constexpr int K = TxOps<G>::K;
+    unsigned long long rw[K], rr[K];
+    uint32_t reads = s.valid & s.isread, writes = s.valid & ~s.isread;
+    uint32_t pending = reads, held = 0;
+    bool fail = false, err = false;
+    uint64_t t0 = gtimer();
+    bool first = true;
+    long long cw = 0;
+    while (true) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (!((pending >> k) & 1u) || err) continue;
+            unsigned long long dt = 0;
+            int r = tictoc_read<SLOW>(p, s.row[k], tx, pos, g.glane + k * G, dt, rw[k], rr[k]);
+            if (r == O_DONE) { pending &= ~(1u << k); dg += dt; }
+            else if (r == O_ERR) err = true;
+        }
+        bool ge = g.any(err), gp = g.any(pending != 0u);
+        if (ge) return kGiveUp;
+        if (!gp) break;
+        if (first) { first = false; cw = clock64(); }
+        if (g.any(expired(t0, p.spin_limit_ns) || error_raised(p.ctr))) {
+            if (g.glane == 0) set_error(p.ctr, GCC_ETIMEOUT, W_TICTOC_READ);
+            return kGiveUp;
+        }
+    }
+    if (!first) ck.wait += clock64() - cw;
+    unsigned long long cts = 0;
+    occ_lock_writes<G, SLOW, true>(p, g, s, writes, ordered, held, cts, fail, err);
+    bool gf = g.any(fail), ge = g.any(err);
+    if (!gf && !ge) {
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            if ((reads >> k) & 1u) cts = cts > rw[k] ? cts : rw[k];
+        cts = g.maxv(cts);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (!((reads >> k) & 1u) || fail || err) continue;
+            if (rr[k] >= cts) continue;
+            int r = tictoc_extend<SLOW>(p, s.row[k], rw[k], cts);
+            if (r == O_FAIL) fail = true;
+            else if (r == O_ERR) err = true;
+        }
+        gf = g.any(fail);
+        ge = g.any(err);
+    }
+    if (gf || ge) {
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            if ((held >> k) & 1u) atomicAnd(p.meta + s.row[k], ~tictoc::kLock);
+        __threadfence();
+        return ge ? kGiveUp : kAbort;
+    }
+    // Serialization key: (batch, commit_ts, order of validation among equal
+    // commit_ts). Within a batch commit_ts <= commits + 1 < 2^32.
+    if ((p.flags & GCC_F_COMMIT_LOG) && g.glane == 0) {
+        p.commit_hi[tx] = p.batch_st;
+        p.commit_lo[tx] = (cts << 32) | (atomicAdd(&p.ctr->seq, 1ull) & 0xFFFFFFFFull);
+    }
+    if (p.write_mode == GCC_WRITE_ROWCOPY) g.sync();
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        if ((writes >> k) & 1u) apply_write(p, s.row[k], tx, pos, g.glane + k * G, s.readmask);
+    __threadfence();
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        if ((writes >> k) & 1u) atomicExch(p.meta + s.row[k], tictoc::make(false, 0, cts));
+    return kCommit;
+}
+
+// ===========================================================================
+// GaccO / GPUTx: deterministic execution in a precomputed order. Each access
+// (row, position p in that row's ordered access list) waits until the row's
+// turn equals p, performs the read or write, and passes the turn to p + 1
+// (gacco.cuh:156-175; GPUTx's rank launches become the same hand-off over the
+// (rank, tx) order, which also orders same-rank conflicts by tx index).
+// ===========================================================================
+template <int G>
+GCC_D int attempt_ordered(const KParams &p, const Group<G> &g, const TxOps<G> &s, uint32_t tx,
+                          uint64_t pos, unsigned long long &dg, Clocks &ck, bool ordered) {
+    constexpr int K = TxOps<G>::K;
+    uint32_t mypos[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        mypos[k] = ((s.valid >> k) & 1u) ? p.op_pos[pos * kMaxOps + g.glane + k * G] : 0u;
+    uint32_t pending = s.valid, done_ops = 0;
+    const bool rowcopy = p.write_mode == GCC_WRITE_ROWCOPY;
+    uint64_t t0 = gtimer();
+    bool first = true;
+    long long cw = 0;
+    while (true) {
+        uint32_t mine = 0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (!((pending >> k) & 1u)) continue;
+            uint32_t i = g.glane + k * G;
+            bool rd = (s.isread >> k) & 1u;
+            if (!rd && rowcopy) {
+                int src = rowcopy_src(s.readmask, i);
+                if (src >= 0 && !((done_ops >> src) & 1u)) continue;
+            }
+            if (ld_volatile(p.turn + s.row[k]) != mypos[k]) continue;
+            __threadfence();
+            if (rd) {
+                read_image(p, row_ptr(p, s.row[k]), tx, pos, i, dg);
+            } else {
+                apply_write(p, s.row[k], tx, pos, i, s.readmask);
+            }
+            __threadfence();
+            atomicExch(p.turn + s.row[k], mypos[k] + 1u);
+            pending &= ~(1u << k);
+            mine |= 1u << i;
+        }
+        done_ops |= g.orv(mine);
+        if (rowcopy) g.sync();
+        if (!g.any(pending != 0u)) break;
+        if (first) { first = false; cw = clock64(); }
+        if (g.any(expired(t0, p.spin_limit_ns) || error_raised(p.ctr))) {
+            if (g.glane == 0) set_error(p.ctr, GCC_ETIMEOUT, W_TURN);
+            return kGiveUp;
+        }
+    }
+    if (!first) ck.wait += clock64() - cw;
+    if ((p.flags & GCC_F_COMMIT_LOG) && g.glane == 0) {
+        p.commit_hi[tx] = p.batch_st + pos;
+        p.commit_lo[tx] = 0ull;
+    }
+    return kCommit;
+}
+
+template <int SCH, int G>
+GCC_D int attempt(const KParams &p, const Group<G> &g, const TxOps<G> &s, uint32_t tx,
+                  uint64_t pos, unsigned long long &dg, Clocks &ck, bool ordered) {
+    if constexpr (SCH == S_TPL_NW) return attempt_tpl<G, false, false>(p, g, s, tx, pos, dg, ck, ordered);
+    else if constexpr (SCH == S_TPL_WD) return attempt_tpl<G, true, false>(p, g, s, tx, pos, dg, ck, ordered);
+    else if constexpr (SCH == S_SLOW_TPL_NW) return attempt_tpl<G, false, true>(p, g, s, tx, pos, dg, ck, ordered);
+    else if constexpr (SCH == S_SLOW_TPL_WD) return attempt_tpl<G, true, true>(p, g, s, tx, pos, dg, ck, ordered);
+    else if constexpr (SCH == S_TO) return attempt_to<G, false>(p, g, s, tx, pos, dg, ck, ordered);
+    else if constexpr (SCH == S_SLOW_TO) return attempt_to<G, true>(p, g, s, tx, pos, dg, ck, ordered);
+    else if constexpr (SCH == S_MVCC) return attempt_mvcc<G, false>(p, g, s, tx, pos, dg, ck, ordered);
+    else if constexpr (SCH == S_SLOW_MVCC) return attempt_mvcc<G, true>(p, g, s, tx, pos, dg, ck, ordered);
+    else if constexpr (SCH == S_SILO) return attempt_silo<G, false>(p, g, s, tx, pos, dg, ck, ordered);
+    else if constexpr (SCH == S_SLOW_SILO) return attempt_silo<G, true>(p, g, s, tx, pos, dg, ck, ordered);
+    else if constexpr (SCH == S_TICTOC) return attempt_tictoc<G, false>(p, g, s, tx, pos, dg, ck, ordered);
+    else if constexpr (SCH == S_SLOW_TICTOC) return attempt_tictoc<G, true>(p, g, s, tx, pos, dg, ck, ordered);
+    else return attempt_ordered<G>(p, g, s, tx, pos, dg, ck, ordered);
+}
+
+__host__ __device__ constexpr bool is_ordered(int s) { return s == S_GACCO || s == S_GPUTX; }
+
+// ===========================================================================
+// The persistent transaction kernel.
+// ===========================================================================
+template <int SCH, int G>
+__global__ void __launch_bounds__(1024, 1) ycsb_kernel(const __grid_constant__ KParams p) {
+    // Block-level histogram and metric sums (flushed once at exit) keep the
+    // per-thread register budget for the transaction itself.
+    __shared__ unsigned s_hist[kHistBuckets];
+    __shared__ unsigned long long s_met[8];
+    for (int i = threadIdx.x; i < kHistBuckets; i += blockDim.x) s_hist[i] = 0u;
+    if (threadIdx.x < 8) s_met[threadIdx.x] = 0ull;
+    __syncthreads();
+
+    const Group<G> g;
+    constexpr int K = TxOps<G>::K;
+
+    while (true) {
+        unsigned long long pos = 0;
+        unsigned stop = 0;
+        if (g.glane == 0) {
+            pos = atomicAdd(&p.ctr->ticket, 1ull);
+            stop = (pos >= p.batch_n || error_raised(p.ctr)) ? 1u : 0u;
+        }
+        stop = g.bcast(stop, 0);
+        if (stop) break;
+        pos = g.bcast(pos, 0);
+        const uint32_t tx = p.order ? __ldg(p.order + p.batch_st + pos) : p.batch_st + (uint32_t)pos;
+        const long long c_start = clock64();
+        const uint64_t t_start = gtimer();
+
+        // ---- requests and index probes --------------------------------
+        TxOps<G> s;
+        const gcc_ycsb_tx *T = p.txs + tx;
+        const unsigned long long n64 = __ldg(&T->request_cnt);
+        if (n64 > (unsigned long long)kMaxOps) {
+            if (g.glane == 0) set_error(p.ctr, GCC_EFORMAT, 0);
+            break;
+        }
+        s.n = (uint32_t)n64;
+        s.valid = s.isread = 0;
+        bool miss = false;
+        uint32_t myreads = 0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const uint32_t i = g.glane + k * G;
+            s.row[k] = kNoRow;
+            if (i < s.n) {
+                const int2 rq = __ldg((const int2 *)&T->requests[i]);
+                s.valid |= 1u << k;
+                if (rq.x) { s.isread |= 1u << k; myreads |= 1u << i; }
+                if constexpr (is_ordered(SCH)) {
+                    s.row[k] = __ldg(p.op_row + pos * kMaxOps + i);
+                } else {
+                    s.row[k] = index_find(p, (uint32_t)rq.y);
+                }
+                miss |= s.row[k] == kNoRow;
+            }
+        }
+        s.readmask = g.orv(myreads);
+        if (g.any(miss)) {
+            if (g.glane == 0) set_error(p.ctr, GCC_EKEY, 0);
+            break;
+        }
+        const long long c_after_idx = clock64();
+
+        // ---- attempt / retry loop (benchmark/ycsb.cu:51-106) -------------
+        unsigned attempts = 0;
+        int st = kGiveUp;
+        Clocks ck{0, 0, 0};
+        unsigned long long dg = 0, c_abort = 0;
+        long long c_attempt = c_after_idx;
+        while (true) {
+            dg = 0;
+            c_attempt = clock64();
+            st = attempt<SCH, G>(p, g, s, tx, pos, dg, ck, attempts > 0);
+            if (st != kAbort) break;
+            ++attempts;
+            c_abort += clock64() - c_attempt;
+            if (g.any(expired(t_start, 4ull * p.spin_limit_ns) || error_raised(p.ctr))) {
+                if (g.glane == 0) set_error(p.ctr, GCC_ETIMEOUT, W_RETRY);
+                st = kGiveUp;
+                break;
+            }
+        }
+        if (st == kGiveUp) break;
+        dg = g.sum(dg);
+        if (g.glane == 0) {
+            const long long c_end = clock64();
+            p.digest[tx] = dg;
+            p.tx_aborts[tx] = attempts;
+            atomicAdd(&s_met[0], 1ull);
+            atomicAdd(&s_met[1], (unsigned long long)attempts);
+            atomicAdd(&s_met[2], ck.ts);
+            atomicAdd(&s_met[3], ck.wait);
+            atomicAdd(&s_met[4], c_abort);
+            atomicAdd(&s_met[5], (unsigned long long)(c_end - c_attempt));
+            atomicAdd(&s_met[6], (unsigned long long)(c_end - c_start));
+            atomicAdd(&s_met[7], (unsigned long long)(c_after_idx - c_start));
+            atomicAdd(&s_hist[hist_bucket(gtimer() - t_start)], 1u);
+        }
+    }
+
+    __syncthreads();
+    if (threadIdx.x < 8 && s_met[threadIdx.x]) {
+        Counters *c = p.ctr;
+        unsigned long long *dst[8] = {&c->committed, &c->aborts, &c->ts_cycles, &c->wait_cycles,
+                                      &c->abort_cycles, &c->mng_cycles, &c->tot_cycles,
+                                      &c->idx_cycles};
+        atomicAdd(dst[threadIdx.x], s_met[threadIdx.x]);
+    }
+    for (int i = threadIdx.x; i < kHistBuckets; i += blockDim.x)
+        if (s_hist[i]) atomicAdd(&p.ctr->hist[i], s_hist[i]);
+}
+
+// Launch helper implemented once per scheme translation unit.
+cudaError_t launch_scheme(int scheme, int G, int grid, int block, const KParams &p,
+                          cudaStream_t stream);
+int occupancy_blocks(int scheme, int G, int block);
+
+}  // namespace gcc

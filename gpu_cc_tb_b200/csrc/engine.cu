@@ -1,0 +1,767 @@
+// engine.cu -- host side of the C ABI: device memory layout, the batch loop,
+// per-scheme metadata resets, GaccO/GPUTx ordering passes and result readout.
+//
+// Reference behaviour followed:
+//   host driver / batch loop            benchmark_cpu/ycsb.cu:81-302
+//   batching into ceil(tx/batch) runs    include/cc.cuh:29-35
+//   per-batch metadata resets            twopl.cuh:431-435, to.cuh:316-321,
+//                                        mvcc.cuh:351-376, silo.cuh:379-383,
+//                                        tictoc.cuh:409-413
+//   GaccO per-batch precompute           include/gacco.cuh:244-339
+//   GPUTx ranking over all transactions  include/gputx.cuh:213-299
+//   metrics + output line                include/runtime.cuh:169-214
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "cc_launch.cuh"
+#include "prep_kernels.cuh"
+
+using namespace gcc;
+
+namespace {
+
+struct SchemeName {
+    const char *name;
+    int id;
+};
+const SchemeName kSchemes[] = {
+    {"tpl_nw", S_TPL_NW},       {"tpl_wd", S_TPL_WD},           {"to", S_TO},
+    {"mvcc", S_MVCC},           {"silo", S_SILO},               {"tictoc", S_TICTOC},
+    {"gacco", S_GACCO},         {"gputx", S_GPUTX},             {"slow_tpl_nw", S_SLOW_TPL_NW},
+    {"slow_tpl_wd", S_SLOW_TPL_WD}, {"slow_to", S_SLOW_TO},     {"slow_mvcc", S_SLOW_MVCC},
+    {"slow_silo", S_SLOW_SILO}, {"slow_tictoc", S_SLOW_TICTOC},
+    // spellings found in the reference's result files / tpcc driver
+    {"slowto", S_SLOW_TO},      {"slowmvcc", S_SLOW_MVCC},
+};
+
+bool is_slow(int s) { return s >= S_SLOW_TPL_NW; }
+bool uses_ts(int s) { return s == S_TO || s == S_SLOW_TO || s == S_MVCC || s == S_SLOW_MVCC; }
+bool is_mvcc(int s) { return s == S_MVCC || s == S_SLOW_MVCC; }
+
+cudaError_t launch_scheme_kernel(int s, int G, int grid, int block, const KParams &p,
+                                 cudaStream_t st) {
+    switch (s) {
+        case S_TPL_NW: case S_TPL_WD: case S_SLOW_TPL_NW: case S_SLOW_TPL_WD:
+            return launch_family_tpl(s, G, grid, block, p, st);
+        case S_TO: case S_SLOW_TO: return launch_family_to(s, G, grid, block, p, st);
+        case S_MVCC: case S_SLOW_MVCC: return launch_family_mvcc(s, G, grid, block, p, st);
+        case S_SILO: case S_SLOW_SILO: return launch_family_silo(s, G, grid, block, p, st);
+        case S_TICTOC: case S_SLOW_TICTOC: return launch_family_tictoc(s, G, grid, block, p, st);
+        default: return launch_family_ordered(s, G, grid, block, p, st);
+    }
+}
+int scheme_occupancy(int s, int G, int block) {
+    switch (s) {
+        case S_TPL_NW: case S_TPL_WD: case S_SLOW_TPL_NW: case S_SLOW_TPL_WD:
+            return occupancy_family_tpl(s, G, block);
+        case S_TO: case S_SLOW_TO: return occupancy_family_to(s, G, block);
+        case S_MVCC: case S_SLOW_MVCC: return occupancy_family_mvcc(s, G, block);
+        case S_SILO: case S_SLOW_SILO: return occupancy_family_silo(s, G, block);
+        case S_TICTOC: case S_SLOW_TICTOC: return occupancy_family_tictoc(s, G, block);
+        default: return occupancy_family_ordered(s, G, block);
+    }
+}
+
+inline unsigned grid1d(uint64_t n, unsigned block) {
+    return (unsigned)((n + block - 1) / block);
+}
+int bits_for(uint64_t maxval) {  // bits to represent 0..maxval
+    int b = 1;
+    while (b < 32 && (1ull << b) <= maxval) ++b;
+    return b;
+}
+
+}  // namespace
+
+#define CK(call)                                   \
+    do {                                           \
+        cudaError_t e_ = (call);                   \
+        if (e_ != cudaSuccess) {                   \
+            last_cuda = e_;                        \
+            return GCC_ECUDA;                      \
+        }                                          \
+    } while (0)
+
+struct gcc_engine {
+    int dev = 0;
+    int sm_count = 0;
+    int clock_khz = 0;
+    cudaStream_t stream = nullptr;
+    cudaError_t last_cuda = cudaSuccess;
+    gcc_table_desc desc{};
+    uint32_t row_bytes = 0, stride = 0, words = 0, wslot = 0;
+    uint64_t rows = 0;
+    uint8_t *table = nullptr;
+    // index
+    unsigned long long *hash_slots = nullptr;
+    uint64_t hash_bucket_mask = 0;
+    unsigned long long *sorted = nullptr;
+    // transactions
+    gcc_ycsb_tx *txs = nullptr;
+    uint64_t n_tx = 0, cap_tx = 0;
+    // per-row metadata
+    unsigned long long *meta = nullptr;
+    unsigned *latch = nullptr;
+    unsigned *turn = nullptr;
+    // per-tx outputs
+    unsigned long long *digest = nullptr, *commit_hi = nullptr, *commit_lo = nullptr;
+    unsigned *tx_aborts = nullptr;
+    uint64_t *read_log = nullptr;
+    uint64_t read_log_units = 0;
+    // per-access scratch (units = positions)
+    uint64_t *scratch = nullptr;
+    uint64_t scratch_units = 0;
+    unsigned long long *ver_ts = nullptr;
+    unsigned *ver_prev = nullptr;
+    uint64_t *ver_data = nullptr;
+    uint64_t ver_units = 0;
+    // ordering passes
+    uint32_t *acc_key[2] = {nullptr, nullptr}, *acc_val[2] = {nullptr, nullptr};
+    uint32_t *op_row = nullptr, *op_pos = nullptr, *order = nullptr, *tx_rank = nullptr;
+    uint32_t *sort_counts = nullptr;
+    uint64_t acc_cap = 0, counts_cap = 0, order_cap = 0;
+    std::vector<uint32_t *> scan_tmp;
+    std::vector<uint64_t> scan_tmp_n;
+    Counters *ctr = nullptr;
+    // timing
+    std::vector<cudaEvent_t> events;
+    double last_kernel_ms = 0;
+    uint64_t last_launches = 0;
+    uint64_t kernel_launches = 0;
+    bool have_run = false;
+
+    ~gcc_engine();
+    int fail_cuda(cudaError_t e) {
+        last_cuda = e;
+        return GCC_ECUDA;
+    }
+    template <class T>
+    int alloc(T **p, size_t bytes) {
+        if (*p) {
+            cudaFree(*p);
+            *p = nullptr;
+        }
+        if (bytes == 0) bytes = 16;
+        cudaError_t e = cudaMalloc((void **)p, bytes);
+        if (e != cudaSuccess) {
+            *p = nullptr;
+            last_cuda = e;
+            cudaGetLastError();
+            return e == cudaErrorMemoryAllocation ? GCC_ENOMEM : GCC_ECUDA;
+        }
+        return GCC_OK;
+    }
+    int ensure_events(size_t n) {
+        while (events.size() < n) {
+            cudaEvent_t ev;
+            CK(cudaEventCreate(&ev));
+            events.push_back(ev);
+        }
+        return GCC_OK;
+    }
+    KParams base_params() const;
+    int radix_sort(uint64_t n, int bits, uint32_t **keys, uint32_t **vals);
+    int scan(const uint32_t *in, uint32_t *out, uint64_t n, bool inclusive, int level = 0);
+    int ensure_access(uint64_t n_acc);
+    int order_pass(const KParams &p, uint64_t n_pos, int sched_bits);
+    int gputx_rank(const KParams &p0);
+};
+
+gcc_engine::~gcc_engine() {
+    if (dev >= 0) cudaSetDevice(dev);
+    void *bufs[] = {table, hash_slots, sorted, txs, meta, latch, turn, digest, commit_hi,
+                    commit_lo, tx_aborts, read_log, scratch, ver_ts, ver_prev, ver_data,
+                    acc_key[0], acc_key[1], acc_val[0], acc_val[1], op_row, op_pos, order,
+                    tx_rank, sort_counts, ctr};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    for (uint32_t *t : scan_tmp)
+        if (t) cudaFree(t);
+    for (cudaEvent_t ev : events) cudaEventDestroy(ev);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+KParams gcc_engine::base_params() const {
+    KParams p;
+    memset(&p, 0, sizeof(p));
+    p.txs = txs;
+    p.n_tx = (uint32_t)n_tx;
+    p.index_kind = desc.index_kind;
+    p.hash_slots = hash_slots;
+    p.hash_bucket_mask = hash_bucket_mask;
+    p.sorted = sorted;
+    p.sorted_len = (uint32_t)rows;
+    p.rows = rows;
+    p.table = table;
+    p.stride = stride;
+    p.words = words;
+    p.wslot = wslot;
+    p.meta = meta;
+    p.latch = latch;
+    p.turn = turn;
+    p.digest = digest;
+    p.commit_hi = commit_hi;
+    p.commit_lo = commit_lo;
+    p.tx_aborts = tx_aborts;
+    p.ctr = ctr;
+    p.spin_limit_ns = 4000000000ull;
+    return p;
+}
+
+// Multi-level exclusive/inclusive scan of u32.
+int gcc_engine::scan(const uint32_t *in, uint32_t *out, uint64_t n, bool inclusive, int level) {
+    if (n == 0) return GCC_OK;
+    uint64_t nb = (n + kScanTile - 1) / kScanTile;
+    if (nb == 1) {
+        k_scan_tile<<<1, kScanThreads, 0, stream>>>(in, out, n, nullptr, inclusive ? 1 : 0);
+        CK(cudaGetLastError());
+        kernel_launches += 1;
+        return GCC_OK;
+    }
+    while ((int)scan_tmp.size() <= level) {
+        scan_tmp.push_back(nullptr);
+        scan_tmp_n.push_back(0);
+    }
+    if (scan_tmp_n[level] < nb) {
+        int rc = alloc(&scan_tmp[level], nb * sizeof(uint32_t));
+        if (rc) return rc;
+        scan_tmp_n[level] = nb;
+    }
+    uint32_t *sums = scan_tmp[level];
+    k_scan_tile<<<(unsigned)nb, kScanThreads, 0, stream>>>(in, out, n, sums, inclusive ? 1 : 0);
+    CK(cudaGetLastError());
+    kernel_launches += 1;
+    int rc = scan(sums, sums, nb, false, level + 1);
+    if (rc) return rc;
+    k_scan_add<<<(unsigned)nb, kScanThreads, 0, stream>>>(out, n, sums);
+    CK(cudaGetLastError());
+    kernel_launches += 1;
+    return GCC_OK;
+}
+
+// Stable LSD radix sort of (keys, vals) over the low `bits` bits; the sorted
+// pair ends in *keys / *vals (buffers may be swapped with the alternates).
+int gcc_engine::radix_sort(uint64_t n, int bits, uint32_t **keys, uint32_t **vals) {
+    if (n == 0) return GCC_OK;
+    uint32_t nblocks = (uint32_t)((n + kSortTile - 1) / kSortTile);
+    uint64_t ncounts = (uint64_t)nblocks * kRadix;
+    if (counts_cap < ncounts) {
+        int rc = alloc(&sort_counts, ncounts * sizeof(uint32_t));
+        if (rc) return rc;
+        counts_cap = ncounts;
+    }
+    uint32_t *ki = *keys, *vi = *vals;
+    uint32_t *ko = (ki == acc_key[0]) ? acc_key[1] : acc_key[0];
+    uint32_t *vo = (vi == acc_val[0]) ? acc_val[1] : acc_val[0];
+    for (int shift = 0; shift < bits; shift += 8) {
+        k_sort_hist<<<nblocks, kSortThreads, 0, stream>>>(ki, n, shift, sort_counts, nblocks);
+        CK(cudaGetLastError());
+        int rc = scan(sort_counts, sort_counts, ncounts, false);
+        if (rc) return rc;
+        k_sort_scatter<<<nblocks, kSortThreads, 0, stream>>>(ki, vi, n, shift, sort_counts,
+                                                              nblocks, ko, vo);
+        CK(cudaGetLastError());
+        kernel_launches += 2;
+        std::swap(ki, ko);
+        std::swap(vi, vo);
+    }
+    *keys = ki;
+    *vals = vi;
+    return GCC_OK;
+}
+
+int gcc_engine::ensure_access(uint64_t n_acc) {
+    if (acc_cap >= n_acc) return GCC_OK;
+    int rc;
+    for (int j = 0; j < 2; ++j) {
+        if ((rc = alloc(&acc_key[j], n_acc * 4))) return rc;
+        if ((rc = alloc(&acc_val[j], n_acc * 4))) return rc;
+    }
+    if ((rc = alloc(&op_row, n_acc * 4))) return rc;
+    if ((rc = alloc(&op_pos, n_acc * 4))) return rc;
+    acc_cap = n_acc;
+    return GCC_OK;
+}
+
+// Access list of positions [p.batch_st, p.batch_st + n_pos) in p.order order:
+// stable sort by row, then per-access positions and each row's first turn.
+int gcc_engine::order_pass(const KParams &p, uint64_t n_pos, int) {
+    uint64_t n_acc = n_pos * kMaxOps;
+    int rc = ensure_access(n_acc);
+    if (rc) return rc;
+    int rbits = bits_for(rows);  // rows itself is the padding key
+    uint32_t invalid = (uint32_t)rows;
+    if (rbits > 32) return GCC_EINVAL;
+    k_access_build<<<grid1d(n_acc, 256), 256, 0, stream>>>(p, n_pos, invalid, acc_key[0],
+                                                           acc_val[0], op_row);
+    CK(cudaGetLastError());
+    kernel_launches += 1;
+    uint32_t *k = acc_key[0], *v = acc_val[0];
+    if ((rc = radix_sort(n_acc, rbits, &k, &v))) return rc;
+    k_access_positions<<<grid1d(n_acc, 256), 256, 0, stream>>>(k, v, n_acc, invalid, op_pos,
+                                                                turn);
+    CK(cudaGetLastError());
+    kernel_launches += 1;
+    return GCC_OK;
+}
+
+// GPUTx ranking (gputx.cuh:213-299, src/gputx.cu:5-38) over all transactions,
+// leaving the (rank, tx) execution order in `order`.
+int gcc_engine::gputx_rank(const KParams &p0) {
+    uint64_t n_acc = n_tx * kMaxOps;
+    int rc = ensure_access(n_acc);
+    if (rc) return rc;
+    if (order_cap < n_tx) {
+        if ((rc = alloc(&order, n_tx * 4))) return rc;
+        if ((rc = alloc(&tx_rank, n_tx * 4))) return rc;
+        order_cap = n_tx;
+    }
+    KParams p = p0;
+    p.order = nullptr;
+    p.batch_st = 0;
+    uint32_t invalid = (uint32_t)rows;
+    int rbits = bits_for(rows);
+    k_access_build<<<grid1d(n_acc, 256), 256, 0, stream>>>(p, n_tx, invalid, acc_key[0],
+                                                           acc_val[0], op_row);
+    CK(cudaGetLastError());
+    uint32_t *k = acc_key[0], *v = acc_val[0];
+    if ((rc = radix_sort(n_acc, rbits, &k, &v))) return rc;
+    // flags -> inclusive scan -> per-row base -> per-tx max rank
+    uint32_t *f = (k == acc_key[0]) ? acc_key[1] : acc_key[0];
+    uint32_t *S = op_pos;  // free until the second ordering pass
+    k_rank_flags<<<grid1d(n_acc, 256), 256, 0, stream>>>(k, v, n_acc, invalid, f);
+    CK(cudaGetLastError());
+    if ((rc = scan(f, S, n_acc, true))) return rc;
+    k_rank_segbase<<<grid1d(n_acc, 256), 256, 0, stream>>>(k, S, n_acc, invalid, turn);
+    CK(cudaGetLastError());
+    CK(cudaMemsetAsync(tx_rank, 0, n_tx * 4, stream));
+    k_rank_tx<<<grid1d(n_acc, 256), 256, 0, stream>>>(k, v, S, n_acc, invalid, turn, tx_rank,
+                                                       &ctr->max_rank);
+    CK(cudaGetLastError());
+    kernel_launches += 4;
+    // stable sort of tx ids by rank: ranks < n_tx
+    uint32_t *rk = (k == acc_key[0]) ? acc_key[1] : acc_key[0];
+    uint32_t *rv = (v == acc_val[0]) ? acc_val[1] : acc_val[0];
+    CK(cudaMemcpyAsync(rk, tx_rank, n_tx * 4, cudaMemcpyDeviceToDevice, stream));
+    k_iota<<<grid1d(n_tx, 256), 256, 0, stream>>>(rv, n_tx);
+    CK(cudaGetLastError());
+    kernel_launches += 1;
+    if ((rc = radix_sort(n_tx, bits_for(n_tx), &rk, &rv))) return rc;
+    CK(cudaMemcpyAsync(order, rv, n_tx * 4, cudaMemcpyDeviceToDevice, stream));
+    return GCC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char *gcc_version(void) { return "gpu_cc_tb_b200 0.1 (sm_100a)"; }
+
+const char *gcc_strerror(int status) {
+    switch (status) {
+        case GCC_OK: return "ok";
+        case GCC_EINVAL: return "invalid argument";
+        case GCC_ENOMEM: return "out of memory";
+        case GCC_ECUDA: return "CUDA runtime error";
+        case GCC_ETIMEOUT: return "bounded device wait timed out";
+        case GCC_EFORMAT: return "malformed transaction record";
+        case GCC_EKEY: return "request key not in index";
+        case GCC_EOVERFLOW: return "timestamp space exhausted";
+        case GCC_ESTATE: return "call out of order";
+        case GCC_ENODEV: return "no usable CUDA device";
+        default: return "unknown status";
+    }
+}
+
+int gcc_scheme_id(const char *name) {
+    if (!name) return GCC_EINVAL;
+    for (const SchemeName &s : kSchemes)
+        if (strcmp(s.name, name) == 0) return s.id;
+    return GCC_EINVAL;
+}
+
+uint32_t gcc_row_bytes(int32_t layout) { return layout == GCC_LAYOUT_REF104 ? 104u : 88u; }
+uint32_t gcc_row_stride(int32_t layout) { return layout == GCC_LAYOUT_REF104 ? 112u : 96u; }
+
+int gcc_create(const gcc_table_desc *d, gcc_engine **out) {
+    if (!d || !out) return GCC_EINVAL;
+    *out = nullptr;
+    if (d->rows == 0 || d->rows >= 0xFFFFFFFFull) return GCC_EINVAL;
+    if (d->layout != GCC_LAYOUT_U64X11 && d->layout != GCC_LAYOUT_REF104) return GCC_EINVAL;
+    if (d->index_kind < GCC_INDEX_HASH || d->index_kind > GCC_INDEX_DIRECT) return GCC_EINVAL;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= d->device || d->device < 0) {
+        cudaGetLastError();
+        return GCC_ENODEV;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, d->device) != cudaSuccess) return GCC_ENODEV;
+    if (prop.major < 10) return GCC_ENODEV;  // built for sm_100a only
+    gcc_engine *e = new gcc_engine();
+    e->dev = d->device;
+    e->desc = *d;
+    if (e->desc.max_batch <= 0) e->desc.max_batch = 65536;
+    e->sm_count = prop.multiProcessorCount;
+    int clk = 0;
+    cudaDeviceGetAttribute(&clk, cudaDevAttrClockRate, d->device);
+    e->clock_khz = clk > 0 ? clk : 1965000;
+    e->rows = d->rows;
+    e->row_bytes = gcc_row_bytes(d->layout);
+    e->stride = gcc_row_stride(d->layout);
+    e->words = e->row_bytes / 8;
+    e->wslot = (e->words + 1) & ~1u;
+    int rc = GCC_OK;
+    auto bail = [&](int r) {
+        delete e;
+        return r;
+    };
+    if (cudaSetDevice(e->dev) != cudaSuccess) return bail(GCC_ENODEV);
+    if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(GCC_ECUDA);
+    if ((rc = e->alloc(&e->table, e->rows * e->stride))) return bail(rc);
+    if ((rc = e->alloc(&e->meta, e->rows * 8))) return bail(rc);
+    if ((rc = e->alloc(&e->turn, e->rows * 4))) return bail(rc);
+    if ((rc = e->alloc(&e->ctr, sizeof(Counters)))) return bail(rc);
+    if (cudaMemsetAsync(e->ctr, 0, sizeof(Counters), e->stream) != cudaSuccess) return bail(GCC_ECUDA);
+    k_fill_table<<<grid1d(e->rows, 256), 256, 0, e->stream>>>(e->table, e->rows, e->stride,
+                                                              e->words, d->layout, d->fill_seed);
+    if (cudaGetLastError() != cudaSuccess) return bail(GCC_ECUDA);
+    if (d->index_kind == GCC_INDEX_HASH) {
+        uint64_t nb = 1;
+        while (nb * 4 < 2 * e->rows) nb <<= 1;  // load factor <= 1/2
+        e->hash_bucket_mask = nb - 1;
+        if ((rc = e->alloc(&e->hash_slots, nb * 4 * 8))) return bail(rc);
+        cudaMemsetAsync(e->hash_slots, 0xFF, nb * 4 * 8, e->stream);
+        k_hash_insert<<<grid1d(e->rows, 256), 256, 0, e->stream>>>(
+            e->table, e->rows, e->stride, e->hash_slots, e->hash_bucket_mask, &e->ctr->err);
+        if (cudaGetLastError() != cudaSuccess) return bail(GCC_ECUDA);
+    } else if (d->index_kind == GCC_INDEX_SORTED) {
+        if ((rc = e->ensure_access(e->rows))) return bail(rc);
+        k_sorted_entries<<<grid1d(e->rows, 256), 256, 0, e->stream>>>(
+            e->table, e->rows, e->stride, e->acc_key[0], e->acc_val[0]);
+        uint32_t *k = e->acc_key[0], *v = e->acc_val[0];
+        if ((rc = e->radix_sort(e->rows, 32, &k, &v))) return bail(rc);
+        if ((rc = e->alloc(&e->sorted, e->rows * 8))) return bail(rc);
+        k_pack_sorted<<<grid1d(e->rows, 256), 256, 0, e->stream>>>(k, v, e->rows, e->sorted);
+        if (cudaGetLastError() != cudaSuccess) return bail(GCC_ECUDA);
+    }
+    unsigned err = 0;
+    if (cudaMemcpyAsync(&err, &e->ctr->err, 4, cudaMemcpyDeviceToHost, e->stream) != cudaSuccess ||
+        cudaStreamSynchronize(e->stream) != cudaSuccess)
+        return bail(GCC_ECUDA);
+    if (err) return bail((int)err);
+    *out = e;
+    return GCC_OK;
+}
+
+void gcc_destroy(gcc_engine *e) { delete e; }
+
+int gcc_load_txs(gcc_engine *e, const gcc_ycsb_tx *txs, uint64_t n_tx) {
+    if (!e || (!txs && n_tx)) return GCC_EINVAL;
+    if (n_tx >= (1ull << 27)) return GCC_EINVAL;  // access ids must fit 31 bits
+    cudaSetDevice(e->dev);
+    int rc;
+    if (e->cap_tx < n_tx) {
+        if ((rc = e->alloc(&e->txs, n_tx * sizeof(gcc_ycsb_tx)))) return rc;
+        if ((rc = e->alloc(&e->digest, n_tx * 8))) return rc;
+        if ((rc = e->alloc(&e->commit_hi, n_tx * 8))) return rc;
+        if ((rc = e->alloc(&e->commit_lo, n_tx * 8))) return rc;
+        if ((rc = e->alloc(&e->tx_aborts, n_tx * 4))) return rc;
+        e->cap_tx = n_tx;
+    }
+    e->n_tx = n_tx;
+    e->have_run = false;
+    if (n_tx) {
+        cudaError_t ce = cudaMemcpyAsync(e->txs, txs, n_tx * sizeof(gcc_ycsb_tx),
+                                         cudaMemcpyHostToDevice, e->stream);
+        if (ce != cudaSuccess) return e->fail_cuda(ce);
+    }
+    return GCC_OK;
+}
+
+int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
+    if (!e || !rp || !out) return GCC_EINVAL;
+    memset(out, 0, sizeof(*out));
+    const int s = gcc_scheme_id(rp->cc_scheme);
+    if (s < 0) return GCC_EINVAL;
+    // knob ranges of benchmark_cpu/ycsb.cu:97-98 (block_size 0 would divide
+    // by zero there, :260-270)
+    if (rp->warp_density < 0 || rp->warp_density > 5) return GCC_EINVAL;
+    if (rp->block_size < 1 || rp->block_size > 32) return GCC_EINVAL;
+    if (rp->batch_size < 1) return GCC_EINVAL;
+    if (rp->write_mode != GCC_WRITE_FIELD && rp->write_mode != GCC_WRITE_ROWCOPY) return GCC_EINVAL;
+    if (!e->txs || e->n_tx == 0) return GCC_ESTATE;
+    cudaSetDevice(e->dev);
+    const int G = 1 << rp->warp_density;
+    const int block = rp->block_size * 32;
+    const bool gputx = s == S_GPUTX;
+    const bool ordered = s == S_GACCO || gputx;
+    const uint64_t batch = gputx ? e->n_tx : std::min<uint64_t>((uint64_t)rp->batch_size, e->n_tx);
+    const uint64_t nbatches = (e->n_tx + batch - 1) / batch;
+    const bool rowcopy = rp->write_mode == GCC_WRITE_ROWCOPY;
+    const bool want_log = (rp->flags & GCC_F_READ_LOG) != 0;
+    int rc;
+
+    // lazily sized per-run buffers
+    if (rowcopy && e->scratch_units < batch) {
+        if ((rc = e->alloc(&e->scratch, batch * kMaxOps * e->wslot * 8))) return rc;
+        e->scratch_units = batch;
+    }
+    if (want_log && e->read_log_units < e->n_tx) {
+        if ((rc = e->alloc(&e->read_log, e->n_tx * kMaxOps * e->wslot * 8))) return rc;
+        e->read_log_units = e->n_tx;
+    }
+    if (is_mvcc(s) && e->ver_units < batch) {
+        if ((rc = e->alloc(&e->ver_ts, batch * kMaxOps * 8))) return rc;
+        if ((rc = e->alloc(&e->ver_prev, batch * kMaxOps * 4))) return rc;
+        if ((rc = e->alloc(&e->ver_data, batch * kMaxOps * e->wslot * 8))) return rc;
+        e->ver_units = batch;
+    }
+    if (is_slow(s) && !e->latch) {
+        if ((rc = e->alloc(&e->latch, e->rows * 4))) return rc;
+        cudaError_t ce = cudaMemsetAsync(e->latch, 0, e->rows * 4, e->stream);
+        if (ce != cudaSuccess) return e->fail_cuda(ce);
+    }
+    if (want_log) {
+        cudaError_t ce = cudaMemsetAsync(e->read_log, 0, e->n_tx * kMaxOps * e->wslot * 8, e->stream);
+        if (ce != cudaSuccess) return e->fail_cuda(ce);
+    }
+
+    int occ = scheme_occupancy(s, G, block);
+    if (occ <= 0) return GCC_EINVAL;  // block too large for this kernel
+    const uint64_t max_grid = (uint64_t)occ * e->sm_count;
+
+    KParams p = e->base_params();
+    p.write_mode = rp->write_mode;
+    p.write_seed = rp->write_seed;
+    p.flags = rp->flags;
+    p.spin_limit_ns = rp->spin_limit_ns ? rp->spin_limit_ns : 4000000000ull;
+    p.wait_die = (s == S_TPL_WD || s == S_SLOW_TPL_WD) ? 1u : 0u;
+    p.scratch = rowcopy ? e->scratch : nullptr;
+    p.read_log = want_log ? e->read_log : nullptr;
+    p.ver_ts = e->ver_ts;
+    p.ver_prev = e->ver_prev;
+    p.ver_data = e->ver_data;
+
+    if ((rc = e->ensure_events(3 * nbatches + 4))) return rc;
+    cudaEvent_t ev_start = e->events[0], ev_pre0 = e->events[1], ev_stop = e->events[2];
+    const uint64_t launches0 = e->kernel_launches;
+
+    cudaStream_t st = e->stream;
+    cudaError_t ce;
+#define CKR(call)                             \
+    do {                                      \
+        ce = (call);                          \
+        if (ce != cudaSuccess) return e->fail_cuda(ce); \
+    } while (0)
+    CKR(cudaMemsetAsync(e->ctr, 0, sizeof(Counters), st));
+    CKR(cudaEventRecord(ev_start, st));
+    // GPUTx ranks every transaction once, before the batches (Init0).
+    if (gputx) {
+        if ((rc = e->gputx_rank(p))) return rc;
+        p.order = e->order;
+    }
+    CKR(cudaEventRecord(ev_pre0, st));
+    for (uint64_t b = 0; b < nbatches; ++b) {
+        cudaEvent_t e0 = e->events[3 + 3 * b], e1 = e->events[4 + 3 * b], e2 = e->events[5 + 3 * b];
+        const uint64_t bst = b * batch;
+        const uint64_t bn = std::min<uint64_t>(batch, e->n_tx - bst);
+        p.batch_st = (uint32_t)bst;
+        p.batch_n = (uint32_t)bn;
+        CKR(cudaEventRecord(e0, st));
+        // per-batch metadata reset (the reference memsets the whole table)
+        const bool keep = (rp->flags & GCC_F_NO_RESET) &&
+                          (s == S_TPL_NW || s == S_TPL_WD || s == S_SILO || s == S_TICTOC ||
+                           s == S_SLOW_TPL_NW || s == S_SLOW_TPL_WD || s == S_SLOW_SILO ||
+                           s == S_SLOW_TICTOC);
+        if (!ordered && !(keep && b > 0)) CKR(cudaMemsetAsync(e->meta, 0, e->rows * 8, st));
+        if (is_mvcc(s)) CKR(cudaMemsetAsync(e->turn, 0xFF, e->rows * 4, st));
+        k_batch_prep<<<1, 1, 0, st>>>(e->ctr, uses_ts(s) ? 1 : 0);
+        CKR(cudaGetLastError());
+        e->kernel_launches += 1;
+        if (s == S_GACCO) {
+            if ((rc = e->order_pass(p, bn, 0))) return rc;
+            p.op_row = e->op_row;
+            p.op_pos = e->op_pos;
+        } else if (gputx) {
+            // second pass: accesses in (rank, tx) order
+            if ((rc = e->order_pass(p, bn, 0))) return rc;
+            p.op_row = e->op_row;
+            p.op_pos = e->op_pos;
+        }
+        CKR(cudaEventRecord(e1, st));
+        uint64_t want = (bn * (uint64_t)G + block - 1) / block;
+        int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, max_grid));
+        CKR(launch_scheme_kernel(s, G, grid, block, p, st));
+        e->kernel_launches += 1;
+        CKR(cudaEventRecord(e2, st));
+    }
+    CKR(cudaEventRecord(ev_stop, st));
+    CKR(cudaStreamSynchronize(st));
+#undef CKR
+
+    Counters hc;
+    ce = cudaMemcpy(&hc, e->ctr, sizeof(Counters), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return e->fail_cuda(ce);
+    e->have_run = true;
+    float ms = 0;
+    double pre_ms = 0, proc_ms = 0;
+    cudaEventElapsedTime(&ms, ev_start, ev_pre0);
+    pre_ms += ms;
+    for (uint64_t b = 0; b < nbatches; ++b) {
+        cudaEventElapsedTime(&ms, e->events[3 + 3 * b], e->events[4 + 3 * b]);
+        pre_ms += ms;
+        cudaEventElapsedTime(&ms, e->events[4 + 3 * b], e->events[5 + 3 * b]);
+        proc_ms += ms;
+    }
+    cudaEventElapsedTime(&ms, ev_start, ev_stop);
+    double tot_ms = ms;
+    e->last_kernel_ms = proc_ms;
+    e->last_launches = nbatches;
+
+    out->committed = hc.committed;
+    out->aborts = hc.aborts;
+    out->pre_s = pre_ms / 1000.0;
+    out->proc_s = proc_ms / 1000.0;
+    out->tot_s = tot_ms / 1000.0;
+    out->tx_per_s = tot_ms > 0 ? (double)hc.committed * 1000.0 / tot_ms : 0.0;
+    const double inv = 1.0 / ((double)e->n_tx * (double)e->clock_khz);
+    out->ts_d = hc.ts_cycles * inv;
+    out->wait_d = hc.wait_cycles * inv;
+    out->abort_d = hc.abort_cycles * inv;
+    out->mng_d = hc.mng_cycles * inv;
+    out->tot_d = hc.tot_cycles * inv;
+    out->idx_d = hc.idx_cycles * inv;
+    out->rank_count = gputx ? hc.max_rank + 1 : 0;
+    out->batches = nbatches;
+    out->kernel_launches = e->kernel_launches - launches0;
+    // latency percentiles from the histogram (bucket upper edges)
+    uint64_t total = 0;
+    for (int i = 0; i < kHistBuckets; ++i) total += hc.hist[i];
+    auto edge = [](int b) -> double {
+        if (b < 16) return (double)b + 1.0;
+        int lg = b / 16 + 3, sub = b % 16;
+        return std::ldexp(16.0 + sub + 1.0, lg - 4);
+    };
+    auto pct = [&](double q) -> double {
+        if (!total) return 0.0;
+        uint64_t target = (uint64_t)std::ceil(q * (double)total), acc = 0;
+        for (int i = 0; i < kHistBuckets; ++i) {
+            acc += hc.hist[i];
+            if (acc >= target) return edge(i) / 1000.0;
+        }
+        return edge(kHistBuckets - 1) / 1000.0;
+    };
+    out->lat_p50_us = pct(0.50);
+    out->lat_p99_us = pct(0.99);
+    if (hc.err) return (int)hc.err;
+    if (hc.committed != e->n_tx) return GCC_ESTATE;
+    return GCC_OK;
+}
+
+int gcc_format_line(const gcc_run_params *p, const gcc_result *r, char *buf, size_t n) {
+    if (!p || !r || !buf || n == 0) return GCC_EINVAL;
+    // ExecInfo::Analyse writes floats through std::ostream (6 significant
+    // digits); the same stream formatting is used here.
+    std::ostringstream of;
+    of << p->cc_scheme << "," << p->warp_density << "," << p->block_size << "," << p->batch_size
+       << "," << (float)r->tx_per_s << "," << r->aborts << "," << (float)r->ts_d << ","
+       << (float)r->wait_d << "," << (float)r->abort_d << "," << (float)r->mng_d << ","
+       << (float)r->tot_d << "," << (float)r->idx_d << "," << (float)r->pre_s << ","
+       << (float)r->proc_s << "," << (float)r->tot_s;
+    std::string str = of.str();
+    if (str.size() + 1 > n) return GCC_EINVAL;
+    memcpy(buf, str.c_str(), str.size() + 1);
+    return GCC_OK;
+}
+
+int gcc_dump_table(gcc_engine *e, void *dst, uint64_t bytes) {
+    if (!e || !dst || bytes < e->rows * e->row_bytes) return GCC_EINVAL;
+    cudaSetDevice(e->dev);
+    cudaError_t ce = cudaMemcpy2DAsync(dst, e->row_bytes, e->table, e->stride, e->row_bytes,
+                                       e->rows, cudaMemcpyDeviceToHost, e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    return ce == cudaSuccess ? GCC_OK : e->fail_cuda(ce);
+}
+
+int gcc_upload_table(gcc_engine *e, const void *src, uint64_t bytes) {
+    if (!e || !src || bytes < e->rows * e->row_bytes) return GCC_EINVAL;
+    cudaSetDevice(e->dev);
+    cudaError_t ce = cudaMemcpy2DAsync(e->table, e->stride, src, e->row_bytes, e->row_bytes,
+                                       e->rows, cudaMemcpyHostToDevice, e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    return ce == cudaSuccess ? GCC_OK : e->fail_cuda(ce);
+}
+
+static int copy_out(gcc_engine *e, void *dst, const void *src, uint64_t bytes) {
+    if (!e->have_run) return GCC_ESTATE;
+    cudaSetDevice(e->dev);
+    cudaError_t ce = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    return ce == cudaSuccess ? GCC_OK : e->fail_cuda(ce);
+}
+
+int gcc_get_digests(gcc_engine *e, uint64_t *dst, uint64_t n) {
+    if (!e || !dst || n > e->n_tx) return GCC_EINVAL;
+    return copy_out(e, dst, e->digest, n * 8);
+}
+
+int gcc_get_tx_aborts(gcc_engine *e, uint32_t *dst, uint64_t n) {
+    if (!e || !dst || n > e->n_tx) return GCC_EINVAL;
+    return copy_out(e, dst, e->tx_aborts, n * 4);
+}
+
+int gcc_get_commit_log(gcc_engine *e, gcc_commit_rec *dst, uint64_t n) {
+    if (!e || !dst || n > e->n_tx) return GCC_EINVAL;
+    std::vector<uint64_t> hi(n), lo(n);
+    int rc = copy_out(e, hi.data(), e->commit_hi, n * 8);
+    if (rc) return rc;
+    if ((rc = copy_out(e, lo.data(), e->commit_lo, n * 8))) return rc;
+    for (uint64_t i = 0; i < n; ++i) dst[i] = gcc_commit_rec{hi[i], lo[i]};
+    return GCC_OK;
+}
+
+int gcc_get_read_log(gcc_engine *e, void *dst, uint64_t bytes) {
+    if (!e || !dst) return GCC_EINVAL;
+    uint64_t need = e->n_tx * kMaxOps * e->wslot * 8;
+    if (!e->read_log || e->read_log_units < e->n_tx) return GCC_ESTATE;
+    if (bytes < need) return GCC_EINVAL;
+    return copy_out(e, dst, e->read_log, need);
+}
+
+int gcc_index_lookup(gcc_engine *e, const uint32_t *keys, uint32_t *rows, uint64_t n) {
+    if (!e || (!keys && n) || (!rows && n)) return GCC_EINVAL;
+    if (n == 0) return GCC_OK;
+    cudaSetDevice(e->dev);
+    uint32_t *dk = nullptr, *dr = nullptr;
+    cudaError_t ce = cudaMalloc(&dk, n * 4);
+    if (ce == cudaSuccess) ce = cudaMalloc(&dr, n * 4);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(dk, keys, n * 4, cudaMemcpyHostToDevice, e->stream);
+    if (ce == cudaSuccess) {
+        KParams p = e->base_params();
+        k_index_lookup<<<grid1d(n, 256), 256, 0, e->stream>>>(p, dk, dr, n);
+        ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(rows, dr, n * 4, cudaMemcpyDeviceToHost, e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    if (dk) cudaFree(dk);
+    if (dr) cudaFree(dr);
+    return ce == cudaSuccess ? GCC_OK : e->fail_cuda(ce);
+}
+
+int gcc_last_kernel_ms(gcc_engine *e, double *kernel_ms, uint64_t *launches) {
+    if (!e || !kernel_ms || !launches) return GCC_EINVAL;
+    if (!e->have_run) return GCC_ESTATE;
+    *kernel_ms = e->last_kernel_ms;
+    *launches = e->last_launches;
+    return GCC_OK;
+}
+
+}  // extern "C"

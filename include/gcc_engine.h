@@ -1,0 +1,192 @@
+/*
+ * gcc_engine.h -- C ABI of the B200 transaction-execution engine.
+ *
+ * The engine executes YCSB transactions on one GPU under the concurrency
+ * control (CC) schemes of the gCCTB testbed. Every entry point below takes
+ * plain pointers and sizes and returns a status code (0 = ok, < 0 = error);
+ * nothing calls exit() and every device-side wait is bounded.
+ *
+ * Reference interfaces replaced (paths inside the gCCTB project):
+ *   - host driver `test_ycsb` main loop          benchmark_cpu/ycsb.cu:81-302
+ *   - CC host base class (Init0/Init/ToGPU/Sync)  include/cc.cuh:18-56
+ *   - device CC duck type (TxStart/Read/Write/TxEnd/Finalize)
+ *                                                  include/cc.cuh:58-88
+ *   - transaction kernel `ycsb`                   benchmark/ycsb.cu:21-111
+ *   - row table + sorted index (Table_CPU::InitData/AddIndex/ToGPU,
+ *     SortedArray_GPU::Find)                       include/table.cuh:61-130,
+ *                                                  include/index.cuh:65-127
+ *   - dataset generator `gen_ycsb`                 generation/gen_ycsb.cu:34-152
+ *   - metrics report ExecInfo::Analyse            include/runtime.cuh:169-214
+ *   - serializability check ExecInfo::Check       src/runtime.cu:129-158
+ *
+ * Threading: one engine is used by one host thread at a time. Separate
+ * engines (on the same or different GPUs) are independent.
+ */
+#ifndef GCC_ENGINE_H
+#define GCC_ENGINE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define GCC_OK 0
+#define GCC_EINVAL (-1)    /* bad argument: unknown scheme, knob out of range */
+#define GCC_ENOMEM (-2)    /* device or host allocation failed */
+#define GCC_ECUDA (-3)     /* a CUDA runtime call failed */
+#define GCC_ETIMEOUT (-4)  /* a bounded device-side wait ran out */
+#define GCC_EFORMAT (-5)   /* malformed transaction record */
+#define GCC_EKEY (-6)      /* a request key is not in the index */
+#define GCC_EOVERFLOW (-7) /* timestamp space of a scheme exhausted */
+#define GCC_ESTATE (-8)    /* call out of order (e.g. run before load) */
+#define GCC_ENODEV (-9)    /* no CUDA device / wrong architecture */
+
+/* ---- table layouts ----------------------------------------------------- */
+/* 88-byte rows: uint64 key + 10 uint64 fields, stored at a 96-byte stride. */
+#define GCC_LAYOUT_U64X11 0
+/* 104-byte rows of gCCTB's `Item` (uint32 id + 10 x char[10],
+ * include/ycsb.cuh:6-19), stored at a 112-byte stride. */
+#define GCC_LAYOUT_REF104 1
+
+/* ---- key -> row indexes ------------------------------------------------ */
+#define GCC_INDEX_HASH 0   /* open addressing, one 32-byte bucket per probe */
+#define GCC_INDEX_SORTED 1 /* sorted (key,row) array + binary search, the
+                              reference's SortedArray_GPU (index.cuh:65-92) */
+#define GCC_INDEX_DIRECT 2 /* key == row id */
+
+/* ---- write semantics --------------------------------------------------- */
+/* A write stores a fresh uint64 into one field; field and value are a pure
+ * function of (write_seed, transaction id, op index). */
+#define GCC_WRITE_FIELD 0
+/* A write copies the transaction-local row buffer (the last row this
+ * transaction read before the write in program order, zeros if none) over
+ * the whole target row: gCCTB's `cc.Write(idx, w_idx, &item, row, sizeof
+ * (Item))` (benchmark/ycsb.cu:84-97). */
+#define GCC_WRITE_ROWCOPY 1
+
+/* ---- run flags --------------------------------------------------------- */
+#define GCC_F_COMMIT_LOG 1u /* record each tx's serialization key */
+#define GCC_F_READ_LOG 2u   /* record every read row image (parity runs) */
+#define GCC_F_NO_RESET 4u   /* keep CC metadata across batches where the
+                               scheme allows it (tpl, silo, tictoc) */
+
+/* Dataset generator dedup modes (gen_ycsb drops repeated keys, which leaves
+ * fewer than 16 requests; resample redraws until 16 distinct keys). */
+#define GCC_DEDUP_DROP 0
+#define GCC_DEDUP_RESAMPLE 1
+
+/* One request of a gen_ycsb record: {int read; unsigned key;} (8 bytes). */
+typedef struct gcc_ycsb_req {
+    int32_t read;
+    uint32_t key;
+} gcc_ycsb_req;
+
+/* One gen_ycsb record: {size_t request_cnt; YCSBReq requests[16];} = 136
+ * bytes, little-endian, headerless array (include/ycsb.cuh:21-33). */
+typedef struct gcc_ycsb_tx {
+    uint64_t request_cnt;
+    gcc_ycsb_req requests[16];
+} gcc_ycsb_tx;
+
+typedef struct gcc_table_desc {
+    uint64_t rows;       /* number of rows (keys 0..rows-1) */
+    int32_t layout;      /* GCC_LAYOUT_* */
+    int32_t index_kind;  /* GCC_INDEX_* */
+    uint64_t fill_seed;  /* fields uniform from this seed; 0 = zero fields */
+    int32_t device;      /* CUDA device ordinal */
+    int32_t max_batch;   /* largest batch_size a run may use (sizes scratch) */
+} gcc_table_desc;
+
+typedef struct gcc_run_params {
+    const char *cc_scheme; /* tpl_nw tpl_wd to mvcc silo tictoc gacco gputx
+                              slow_tpl_nw slow_tpl_wd slow_to slow_mvcc
+                              slow_silo slow_tictoc (+ aliases slowto,
+                              slowmvcc) */
+    int32_t warp_density;  /* 2^wd threads per transaction, 0..5 */
+    int32_t block_size;    /* warps per CTA, 1..32 */
+    int32_t batch_size;    /* transactions per batch (gputx ranks all) */
+    uint32_t flags;        /* GCC_F_* */
+    int32_t write_mode;    /* GCC_WRITE_* */
+    int32_t reserved;
+    uint64_t write_seed;   /* seed of GCC_WRITE_FIELD values */
+    uint64_t spin_limit_ns;/* bound of any single device wait; 0 = 4 s */
+} gcc_run_params;
+
+/* Fields 1-15 are the 15 columns of the reference's output line
+ * (include/runtime.cuh:182-196); *_d are per-transaction averages in ms of
+ * GPU clock, *_s are seconds of host-observed (CUDA event) time. */
+typedef struct gcc_result {
+    double tx_per_s;
+    uint64_t committed;
+    uint64_t aborts;
+    double ts_d, wait_d, abort_d, mng_d, tot_d, idx_d;
+    double pre_s, proc_s, tot_s;
+    double lat_p50_us, lat_p99_us; /* per-tx first start -> commit */
+    uint64_t rank_count;           /* gputx: number of ranks */
+    uint64_t batches;              /* kernel batches launched */
+    uint64_t kernel_launches;      /* engine kernels launched by the run */
+} gcc_result;
+
+/* Serialization key of one committed transaction: replaying transactions in
+ * ascending (hi, lo) order reproduces the run. */
+typedef struct gcc_commit_rec {
+    uint64_t hi;
+    uint64_t lo;
+} gcc_commit_rec;
+
+typedef struct gcc_engine gcc_engine;
+
+/* Library / device information. */
+const char *gcc_version(void);
+const char *gcc_strerror(int status);
+int gcc_scheme_id(const char *cc_scheme); /* >= 0, or GCC_EINVAL */
+uint32_t gcc_row_bytes(int32_t layout);   /* 88 or 104 */
+uint32_t gcc_row_stride(int32_t layout);  /* 96 or 112 */
+
+/* Dataset generation (host; gen_ycsb, generation/gen_ycsb.cu:34-152).
+ * Keys are Zipfian (Gray et al. 1994) ranks: key_base 1 draws keys in
+ * [1, rows-1] exactly like gen_ycsb; key_base 0 draws in [0, rows-1].
+ * Deterministic in (seed, tx index); `threads` host threads (0 = all). */
+int gcc_gen_ycsb(uint64_t rows, uint64_t n_tx, double theta, double read_ratio,
+                 uint64_t seed, int32_t dedup, int32_t key_base,
+                 int32_t threads, gcc_ycsb_tx *out);
+
+/* Engine lifetime (Table_CPU::InitData + AddIndex + DB_CPU::ToGPU). */
+int gcc_create(const gcc_table_desc *desc, gcc_engine **out);
+void gcc_destroy(gcc_engine *e);
+
+/* Upload n_tx gen_ycsb records from host memory (benchmark_cpu/ycsb.cu:
+ * 120-148). Records are validated on the device (request_cnt <= 16). */
+int gcc_load_txs(gcc_engine *e, const gcc_ycsb_tx *txs, uint64_t n_tx);
+
+/* Execute every loaded transaction under one scheme (the batch loop of
+ * benchmark_cpu/ycsb.cu:249-292). Synchronous. */
+int gcc_run(gcc_engine *e, const gcc_run_params *p, gcc_result *out);
+
+/* Reference output line (ExecInfo::Analyse CSV columns) for a result. */
+int gcc_format_line(const gcc_run_params *p, const gcc_result *r, char *buf,
+                    size_t buf_bytes);
+
+/* Results of the last run / current state (device -> host copies). */
+int gcc_dump_table(gcc_engine *e, void *host_dst, uint64_t bytes); /* packed rows */
+int gcc_upload_table(gcc_engine *e, const void *host_src, uint64_t bytes);
+int gcc_get_digests(gcc_engine *e, uint64_t *dst, uint64_t n_tx);
+int gcc_get_commit_log(gcc_engine *e, gcc_commit_rec *dst, uint64_t n_tx);
+int gcc_get_tx_aborts(gcc_engine *e, uint32_t *dst, uint64_t n_tx);
+/* Read log: n_tx * 16 row images of row_bytes each (slot = tx*16 + op). */
+int gcc_get_read_log(gcc_engine *e, void *dst, uint64_t bytes);
+/* Index probe for n keys (testing the index): rows[i] = row or UINT32_MAX. */
+int gcc_index_lookup(gcc_engine *e, const uint32_t *keys, uint32_t *rows,
+                     uint64_t n);
+
+/* Device-side timing of the last run's main kernels: total ms and number of
+ * launches of the transaction kernel (for roofline accounting). */
+int gcc_last_kernel_ms(gcc_engine *e, double *kernel_ms, uint64_t *launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GCC_ENGINE_H */

@@ -1,0 +1,132 @@
+"""ctypes loader of the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE: imported only by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, always as the checker or the timed CPU
+baseline, never as part of the engine.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+_lib = None
+
+
+def build():
+    src = [HERE / "oracle.cpp", HERE / "oracle.h"]
+    if not LIB.exists() or LIB.stat().st_mtime < max(p.stat().st_mtime for p in src):
+        subprocess.run(["make", "-C", str(HERE), "-s"], check=True)
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(str(LIB))
+        P, U64, I32 = C.c_void_p, C.c_uint64, C.c_int32
+        sig = {
+            "oracle_fill_table": [U64, I32, U64, P],
+            "oracle_replay": [P, U64, I32, P, U64, P, U64, I32, U64, P, P],
+            "oracle_gputx_order": [P, U64, U64, P, P, P],
+            "oracle_commit_order": [P, U64, P],
+            "oracle_conflict_acyclic": [P, U64, U64],
+            "oracle_cpu_run": [C.c_char_p, P, U64, I32, P, U64, I32, U64, I32, P, P,
+                               C.POINTER(C.c_double), C.POINTER(U64)],
+            "oracle_gen_ycsb": [U64, U64, C.c_double, C.c_double, U64, I32, I32, P],
+        }
+        for name, args in sig.items():
+            fn = getattr(L, name)
+            fn.restype = C.c_int
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def rbytes(layout):
+    return 104 if layout == 1 else 88
+
+
+def rstride(layout):
+    return 112 if layout == 1 else 96
+
+
+def fill_table(rows, layout, seed):
+    t = np.empty((rows, rbytes(layout)), dtype=np.uint8)
+    rc = lib().oracle_fill_table(rows, layout, seed, _p(t))
+    assert rc == 0, rc
+    return t
+
+
+def replay(table, layout, txs, order, write_mode, write_seed, read_log=False):
+    """Serially execute txs[order] over a copy of `table`; returns
+    (final_table, digests[n_tx], read_log or None). Txs not in `order` keep
+    digest 0."""
+    t = np.array(table, dtype=np.uint8, copy=True)
+    n = len(txs)
+    dg = np.zeros(n, dtype=np.uint64)
+    order = np.ascontiguousarray(np.arange(n) if order is None else order, dtype=np.uint32)
+    rl = np.zeros((n, 16, rstride(layout)), dtype=np.uint8) if read_log else None
+    rc = lib().oracle_replay(_p(t), t.shape[0], layout, _p(txs), n, _p(order), len(order),
+                             write_mode, write_seed, _p(dg), _p(rl))
+    if rc != 0:
+        raise RuntimeError(f"oracle_replay failed: {rc}")
+    return t, dg, rl
+
+
+def gputx_order(txs, rows):
+    n = len(txs)
+    ranks = np.zeros(n, dtype=np.uint32)
+    order = np.zeros(n, dtype=np.uint32)
+    mx = np.zeros(1, dtype=np.uint32)
+    rc = lib().oracle_gputx_order(_p(txs), n, rows, _p(ranks), _p(order), _p(mx))
+    assert rc == 0, rc
+    return ranks, order, int(mx[0])
+
+
+def commit_order(log):
+    log = np.ascontiguousarray(log, dtype=np.uint64)
+    order = np.zeros(len(log), dtype=np.uint32)
+    rc = lib().oracle_commit_order(_p(log), len(log), _p(order))
+    assert rc == 0
+    return order
+
+
+EVENT_DTYPE = np.dtype([("tx", "<u4"), ("row", "<u4"), ("is_write", "<u4"), ("pad", "<u4"),
+                        ("seq", "<u8")])
+
+
+def conflict_acyclic(events, n_tx):
+    ev = np.ascontiguousarray(events, dtype=EVENT_DTYPE)
+    return bool(lib().oracle_conflict_acyclic(_p(ev), len(ev), n_tx))
+
+
+def cpu_run(scheme, table, layout, txs, write_mode, write_seed, threads=0, commit_log=True):
+    t = np.array(table, dtype=np.uint8, copy=True)
+    n = len(txs)
+    dg = np.zeros(n, dtype=np.uint64)
+    log = np.zeros((n, 2), dtype=np.uint64) if commit_log else None
+    secs, aborts = C.c_double(), C.c_uint64()
+    rc = lib().oracle_cpu_run(scheme.encode(), _p(t), t.shape[0], layout, _p(txs), n, write_mode,
+                              write_seed, threads, _p(dg), _p(log), C.byref(secs),
+                              C.byref(aborts))
+    if rc != 0:
+        raise RuntimeError(f"oracle_cpu_run failed: {rc}")
+    return t, dg, log, secs.value, aborts.value
+
+
+def gen_ycsb(rows, n_tx, theta, read_ratio, seed, dedup, key_base):
+    from gpu_cc_tb_b200 import TX_DTYPE
+    out = np.zeros(n_tx, dtype=TX_DTYPE)
+    rc = lib().oracle_gen_ycsb(rows, n_tx, theta, read_ratio, seed, dedup, key_base, _p(out))
+    assert rc == 0, rc
+    return out
