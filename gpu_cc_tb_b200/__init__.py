@@ -64,7 +64,7 @@ class TableDesc(C.Structure):
 class RunParams(C.Structure):
     _fields_ = [("cc_scheme", C.c_char_p), ("warp_density", C.c_int32),
                 ("block_size", C.c_int32), ("batch_size", C.c_int32), ("flags", C.c_uint32),
-                ("write_mode", C.c_int32), ("reserved", C.c_int32), ("write_seed", C.c_uint64),
+                ("write_mode", C.c_int32), ("backoff_ns", C.c_int32), ("write_seed", C.c_uint64),
                 ("spin_limit_ns", C.c_uint64)]
 
 
@@ -75,7 +75,8 @@ class Result(C.Structure):
                 ("pre_s", C.c_double), ("proc_s", C.c_double), ("tot_s", C.c_double),
                 ("lat_p50_us", C.c_double), ("lat_p99_us", C.c_double),
                 ("rank_count", C.c_uint64), ("batches", C.c_uint64),
-                ("kernel_launches", C.c_uint64)]
+                ("kernel_launches", C.c_uint64), ("max_attempts", C.c_uint32),
+                ("err_site", C.c_uint32)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -114,6 +115,8 @@ def library() -> C.CDLL:
         "gcc_destroy": (None, [P]),
         "gcc_load_txs": (C.c_int, [P, P, C.c_uint64]),
         "gcc_run": (C.c_int, [P, C.POINTER(RunParams), C.POINTER(Result)]),
+        "gcc_run_checked": (C.c_int, [P, C.POINTER(RunParams), C.POINTER(Result),
+                                      C.POINTER(C.c_int)]),
         "gcc_format_line": (C.c_int, [C.POINTER(RunParams), C.POINTER(Result), C.c_char_p,
                                       C.c_size_t]),
         "gcc_dump_table": (C.c_int, [P, P, C.c_uint64]),
@@ -204,21 +207,33 @@ class Engine:
 
     def params(self, scheme: str, warp_density: int = 5, block_size: int = 32,
                batch_size: int = 65536, flags: int = 0, write_mode: int = WRITE_FIELD,
-               write_seed: int = 1, spin_limit_ns: int = 0) -> RunParams:
+               write_seed: int = 1, spin_limit_ns: int = 0, backoff_ns: int = 0) -> RunParams:
         self._scheme = scheme.encode()
-        return RunParams(self._scheme, warp_density, block_size, batch_size, flags, write_mode, 0,
-                         write_seed, spin_limit_ns)
+        return RunParams(self._scheme, warp_density, block_size, batch_size, flags, write_mode,
+                         backoff_ns, write_seed, spin_limit_ns)
 
     def run(self, scheme: str, **kw) -> dict:
         p = self.params(scheme, **kw)
         r = Result()
         rc = self.lib.gcc_run(self._h, C.byref(p), C.byref(r))
-        _check(rc, f"gcc_run({scheme})")
+        self.last_result = r.as_dict()
+        _check(rc, f"gcc_run({scheme}) err_site={r.err_site} max_attempts={r.max_attempts}")
         out = r.as_dict()
         buf = C.create_string_buffer(512)
         _check(self.lib.gcc_format_line(C.byref(p), C.byref(r), buf, 512), "gcc_format_line")
         out["line"] = buf.value.decode()
         return out
+
+    def run_checked(self, scheme: str, **kw) -> tuple[dict, bool]:
+        """Run, then re-execute the committed transactions in their recorded
+        serialization order on the GPU; returns (result, serializable)."""
+        p = self.params(scheme, **kw)
+        r = Result()
+        v = C.c_int(-1)
+        rc = self.lib.gcc_run_checked(self._h, C.byref(p), C.byref(r), C.byref(v))
+        self.last_result = r.as_dict()
+        _check(rc, f"gcc_run_checked({scheme})")
+        return r.as_dict(), v.value == 1
 
     def dump_table(self) -> np.ndarray:
         a = np.empty((self.rows, self.row_bytes), dtype=np.uint8)

@@ -99,6 +99,9 @@ struct TxOps {
 
 // Bounded wait helper: true once `limit` ns have passed since `t0`.
 GCC_D bool expired(uint64_t t0, uint64_t limit) { return gtimer() - t0 > limit; }
+// Pause inside a wait loop so that diverged lanes of the same warp (another
+// transaction's group, possibly the one being waited for) get issue slots.
+GCC_D void wait_pause() { __nanosleep(20); }
 
 // ---------------------------------------------------------------------------
 // Row images: digest, read log, rowcopy scratch, writes.
@@ -163,11 +166,15 @@ GCC_D void apply_write(const KParams &p, uint32_t row, uint32_t tx, uint64_t pos
 // Latches of the slow_* variants (runtime.cuh:91-109), bounded.
 // ---------------------------------------------------------------------------
 GCC_D bool latch_acquire(const KParams &p, uint32_t row) {
+    // CAS spin as in latch_lock (include/runtime.cuh:91-96), bounded. (A
+    // test-and-test-and-set spin on a plain load starved diverged holder
+    // lanes of the same warp here; every CAS attempt keeps the spinning path
+    // stalled on L2 long enough for the holder to run its release.)
     unsigned *l = p.latch + row;
-    if (atomicCAS(l, 0u, 1u) == 0u) { __threadfence(); return true; }
+    if (atomicCAS(l, 0u, 1u) == 0u) { fence_acq_rel(); return true; }
     uint64_t t0 = gtimer();
     while (true) {
-        if (atomicCAS(l, 0u, 1u) == 0u) { __threadfence(); return true; }
+        if (atomicCAS(l, 0u, 1u) == 0u) { fence_acq_rel(); return true; }
         if (expired(t0, p.spin_limit_ns) || error_raised(p.ctr)) {
             set_error(p.ctr, GCC_ETIMEOUT, W_LATCH);
             return false;
@@ -175,7 +182,7 @@ GCC_D bool latch_acquire(const KParams &p, uint32_t row) {
     }
 }
 GCC_D void latch_release(const KParams &p, uint32_t row) {
-    __threadfence();
+    fence_acq_rel();
     atomicExch(p.latch + row, 0u);
 }
 
@@ -253,7 +260,7 @@ GCC_D bool tpl_unlock(const KParams &p, uint32_t row, bool shared) {
     } else {
         // the exclusive holder is the only writer of the word
         // (slow_twopl.cuh:333-338 stores without the latch)
-        __threadfence();
+        fence_acq_rel();
         atomicExch(p.meta + row, 0ull);
     }
     return true;
@@ -291,6 +298,7 @@ GCC_D int attempt_tpl(const KParams &p, const Group<G> &g, const TxOps<G> &s, ui
                         r = tpl_lock<WD, SLOW>(p, s.row[k], tx, (s.isread >> k) & 1u);
                         if (r != L_WAIT) break;
                         if (first) { first = false; cw = clock64(); }
+        wait_pause();
                         if (expired(t0, p.spin_limit_ns) || error_raised(p.ctr)) {
                             set_error(p.ctr, GCC_ETIMEOUT, W_TPL_WD);
                             r = L_ERR;
@@ -318,6 +326,7 @@ GCC_D int attempt_tpl(const KParams &p, const Group<G> &g, const TxOps<G> &s, ui
             if (ge) { fail = true; err = true; break; }
             if (gf || !gp) { fail = gf; break; }
             if (first) { first = false; cw = clock64(); }
+        wait_pause();
             if (g.any(expired(t0, p.spin_limit_ns) || error_raised(p.ctr))) {
                 if (g.glane == 0) set_error(p.ctr, GCC_ETIMEOUT, W_TPL_WD);
                 fail = true; err = true; break;
@@ -331,11 +340,18 @@ GCC_D int attempt_tpl(const KParams &p, const Group<G> &g, const TxOps<G> &s, ui
             if ((held >> k) & 1u) tpl_unlock<SLOW>(p, s.row[k], (s.isread >> k) & 1u);
         return err ? kGiveUp : kAbort;
     }
-    __threadfence();
-    // Serialization point: every lock is held.
-    if ((p.flags & GCC_F_COMMIT_LOG) && g.glane == 0) {
-        p.commit_hi[tx] = atomicAdd(&p.ctr->seq, 1ull);
-        p.commit_lo[tx] = 0ull;
+    fence_acq_rel();
+    // Serialization point: every lock is held. The leader's sequence number
+    // is ordered after every lane's acquisition and before every lane's
+    // release by the two warp syncs (lanes' memory operations are otherwise
+    // unordered with respect to each other).
+    if (p.flags & GCC_F_COMMIT_LOG) {
+        g.sync();
+        if (g.glane == 0) {
+            p.commit_hi[tx] = atomicAdd(&p.ctr->seq, 1ull);
+            p.commit_lo[tx] = 0ull;
+        }
+        g.sync();
     }
 #pragma unroll
     for (int k = 0; k < K; ++k) {
@@ -348,7 +364,7 @@ GCC_D int attempt_tpl(const KParams &p, const Group<G> &g, const TxOps<G> &s, ui
     for (int k = 0; k < K; ++k)
         if (((s.valid & ~s.isread) >> k) & 1u)
             apply_write(p, s.row[k], tx, pos, (uint32_t)(g.glane + k * G), s.readmask);
-    __threadfence();
+    fence_acq_rel();
     bool uerr = false;
 #pragma unroll
     for (int k = 0; k < K; ++k)
@@ -386,7 +402,7 @@ GCC_D int to_read(const KParams &p, uint32_t row, uint64_t ts, uint32_t tx, uint
     read_image(p, row_ptr(p, row), tx, pos, i, dt);
     if (tso::rts(x) >= ts) {
         // rts already covers this reader: only check the snapshot held
-        __threadfence();
+        fence_acq_rel();
         return ld_cg(m) == x ? O_DONE : O_RETRY;
     }
     unsigned long long nx = tso::make(false, ts, tso::wts(x));
@@ -432,31 +448,68 @@ GCC_D int attempt_to(const KParams &p, const Group<G> &g, const TxOps<G> &s, uin
     uint64_t t0 = gtimer();
     bool first = true;
     long long cw = 0;
-    while (true) {
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            if (!((pending >> k) & 1u) || fail || err) continue;
-            uint32_t i = g.glane + k * G;
-            int r;
-            if ((s.isread >> k) & 1u) {
-                unsigned long long dt = 0;
-                r = to_read<SLOW>(p, s.row[k], ts, tx, pos, i, dt);
-                if (r == O_DONE) dg += dt;
-            } else {
-                r = to_write<SLOW>(p, s.row[k], ts, prev[k]);
-                if (r == O_DONE) wrote |= 1u << k;
-            }
-            if (r == O_DONE) pending &= ~(1u << k);
-            else if (r == O_FAIL) fail = true;
-            else if (r == O_ERR) err = true;
+    // One request: read (waits while an older writer's version is
+    // uncommitted) or write (marks the row uncommitted with this ts).
+    auto op = [&](int k) -> int {
+        const uint32_t i = g.glane + k * G;
+        int r;
+        if ((s.isread >> k) & 1u) {
+            unsigned long long dt = 0;
+            r = to_read<SLOW>(p, s.row[k], ts, tx, pos, i, dt);
+            if (r == O_DONE) dg += dt;
+        } else {
+            r = to_write<SLOW>(p, s.row[k], ts, prev[k]);
+            if (r == O_DONE) wrote |= 1u << k;
         }
-        bool ge = g.any(err), gf = g.any(fail), gp = g.any(pending != 0u);
-        if (ge) { fail = err = true; break; }
-        if (gf || !gp) { fail = gf; break; }
-        if (first) { first = false; cw = clock64(); }
-        if (g.any(expired(t0, p.spin_limit_ns) || error_raised(p.ctr))) {
-            if (g.glane == 0) set_error(p.ctr, GCC_ETIMEOUT, W_TO_READ);
-            fail = err = true; break;
+        return r;
+    };
+    if (ordered) {
+        // Retries visit the requests one at a time in request (= ascending
+        // key) order like the reference, so two writers cannot keep holding
+        // each other's rows uncommitted and aborting each other.
+        for (uint32_t i = 0; i < s.n && !fail; ++i) {
+            const int owner = (int)(i % G), kk = (int)(i / G);
+            int r = O_DONE;
+            if (g.glane == owner) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    if (k != kk) continue;
+                    while (true) {
+                        r = op(k);
+                        if (r != O_RETRY) break;
+                        if (first) { first = false; cw = clock64(); }
+        wait_pause();
+                        if (expired(t0, p.spin_limit_ns) || error_raised(p.ctr)) {
+                            set_error(p.ctr, GCC_ETIMEOUT, W_TO_READ);
+                            r = O_ERR;
+                            break;
+                        }
+                    }
+                }
+            }
+            r = g.bcast(r, owner);
+            if (r == O_FAIL) fail = true;
+            else if (r == O_ERR) fail = err = true;
+        }
+    } else {
+        while (true) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                if (!((pending >> k) & 1u) || fail || err) continue;
+                int r = op(k);
+                if (r == O_DONE) pending &= ~(1u << k);
+                else if (r == O_FAIL) fail = true;
+                else if (r == O_ERR) err = true;
+            }
+            bool ge = g.any(err), gf = g.any(fail), gp = g.any(pending != 0u);
+            if (ge) { fail = err = true; break; }
+            if (gf || !gp) { fail = gf; break; }
+            if (first) { first = false; cw = clock64(); }
+        wait_pause();
+            if (g.any(expired(t0, p.spin_limit_ns) || error_raised(p.ctr))) {
+                if (g.glane == 0) set_error(p.ctr, GCC_ETIMEOUT, W_TO_READ);
+                fail = err = true; break;
+            }
         }
     }
     if (!first) ck.wait += clock64() - cw;
@@ -465,7 +518,7 @@ GCC_D int attempt_to(const KParams &p, const Group<G> &g, const TxOps<G> &s, uin
 #pragma unroll
         for (int k = 0; k < K; ++k)
             if ((wrote >> k) & 1u) atomicExch(p.meta + s.row[k], prev[k]);
-        __threadfence();
+        fence_acq_rel();
         return err ? kGiveUp : kAbort;
     }
     // Serialization key: (batch, timestamp); timestamps restart per batch.
@@ -477,7 +530,7 @@ GCC_D int attempt_to(const KParams &p, const Group<G> &g, const TxOps<G> &s, uin
 #pragma unroll
     for (int k = 0; k < K; ++k)
         if ((wrote >> k) & 1u) apply_write(p, s.row[k], tx, pos, g.glane + k * G, s.readmask);
-    __threadfence();
+    fence_acq_rel();
 #pragma unroll
     for (int k = 0; k < K; ++k)
         if ((wrote >> k) & 1u) atomicExch(p.meta + s.row[k], tso::make(false, ts, ts));
@@ -504,7 +557,7 @@ GCC_D int mvcc_read(const KParams &p, uint32_t row, uint64_t ts, uint32_t tx, ui
     } else if (tso::wts(x) <= ts) {
         read_image(p, row_ptr(p, row), tx, pos, i, dt);
         if (tso::rts(x) >= ts) {
-            __threadfence();
+            fence_acq_rel();
             r = (SLOW || ld_cg(m) == x) ? O_DONE : O_RETRY;
         } else if (SLOW) {
             *(volatile unsigned long long *)m = tso::make(false, ts, tso::wts(x));
@@ -525,7 +578,7 @@ GCC_D int mvcc_read(const KParams &p, uint32_t row, uint64_t ts, uint32_t tx, ui
             r = O_ERR;
         } else {
             read_image(p, p.ver_data + (size_t)node * p.wslot, tx, pos, i, dt);
-            __threadfence();
+            fence_acq_rel();
             r = (SLOW || ld_cg(m) == x) ? O_DONE : O_RETRY;
         }
     }
@@ -573,6 +626,7 @@ GCC_D int attempt_mvcc(const KParams &p, const Group<G> &g, const TxOps<G> &s, u
                     if (r == O_DONE) break;
                     if (r == O_FAIL) { fail = true; break; }
                     if (r == O_ERR) { err = true; break; }
+                    wait_pause();
                     if (expired(t0, p.spin_limit_ns) || error_raised(p.ctr)) {
                         set_error(p.ctr, GCC_ETIMEOUT, W_MVCC_READ);
                         err = true;
@@ -589,7 +643,7 @@ GCC_D int attempt_mvcc(const KParams &p, const Group<G> &g, const TxOps<G> &s, u
 #pragma unroll
         for (int k = 0; k < K; ++k)
             if ((wrote >> k) & 1u) atomicExch(p.meta + s.row[k], prev[k]);
-        __threadfence();
+        fence_acq_rel();
         return err ? kGiveUp : kAbort;
     }
     // Serialization key: (batch, timestamp); timestamps restart per batch.
@@ -609,10 +663,10 @@ GCC_D int attempt_mvcc(const KParams &p, const Group<G> &g, const TxOps<G> &s, u
         copy_image(p, p.ver_data + (size_t)node * p.wslot, row_ptr(p, row));
         p.ver_ts[node] = prev[k];
         p.ver_prev[node] = ld_cg(p.turn + row);
-        __threadfence();
+        fence_acq_rel();
         atomicExch(p.turn + row, node);
         apply_write(p, row, tx, pos, i, s.readmask);
-        __threadfence();
+        fence_acq_rel();
         atomicExch(p.meta + row, tso::make(false, ts, ts));
     }
     return kCommit;
@@ -638,9 +692,9 @@ GCC_D int silo_read(const KParams &p, uint32_t row, uint32_t tx, uint64_t pos, u
     }
     unsigned long long x1 = ld_cg(m);
     if (x1 & silo::kLock) return O_RETRY;
-    __threadfence();
+    fence_acq_rel();
     read_image(p, row_ptr(p, row), tx, pos, i, dt);
-    __threadfence();
+    fence_acq_rel();
     unsigned long long x2 = ld_cg(m);
     if (x1 != x2) return O_RETRY;
     ts = silo::ts(x1);
@@ -739,6 +793,7 @@ GCC_D int attempt_silo(const KParams &p, const Group<G> &g, const TxOps<G> &s, u
         if (ge) return kGiveUp;
         if (!gp) break;
         if (first) { first = false; cw = clock64(); }
+        wait_pause();
         if (g.any(expired(t0, p.spin_limit_ns) || error_raised(p.ctr))) {
             if (g.glane == 0) set_error(p.ctr, GCC_ETIMEOUT, W_SILO_READ);
             return kGiveUp;
@@ -750,11 +805,17 @@ GCC_D int attempt_silo(const KParams &p, const Group<G> &g, const TxOps<G> &s, u
     occ_lock_writes<G, SLOW, false>(p, g, s, writes, ordered, held, cts, fail, err);
     bool gf = g.any(fail), ge = g.any(err);
     if (!gf && !ge) {
-        __threadfence();
-        // Serialization point: write set locked, read set not yet validated.
-        if ((p.flags & GCC_F_COMMIT_LOG) && g.glane == 0) {
-            p.commit_hi[tx] = atomicAdd(&p.ctr->seq, 1ull);
-            p.commit_lo[tx] = 0ull;
+        fence_acq_rel();
+        // Serialization point: write set locked (by every lane), read set not
+        // yet validated (by any lane); the warp syncs order the leader's
+        // sequence number between the two.
+        if (p.flags & GCC_F_COMMIT_LOG) {
+            g.sync();
+            if (g.glane == 0) {
+                p.commit_hi[tx] = atomicAdd(&p.ctr->seq, 1ull);
+                p.commit_lo[tx] = 0ull;
+            }
+            g.sync();
         }
 #pragma unroll
         for (int k = 0; k < K; ++k) {
@@ -769,7 +830,7 @@ GCC_D int attempt_silo(const KParams &p, const Group<G> &g, const TxOps<G> &s, u
 #pragma unroll
         for (int k = 0; k < K; ++k)
             if ((held >> k) & 1u) atomicAnd(p.meta + s.row[k], ~silo::kLock);
-        __threadfence();
+        fence_acq_rel();
         return ge ? kGiveUp : kAbort;
     }
     cts = g.maxv(cts) + 1ull;
@@ -777,7 +838,7 @@ GCC_D int attempt_silo(const KParams &p, const Group<G> &g, const TxOps<G> &s, u
 #pragma unroll
     for (int k = 0; k < K; ++k)
         if ((writes >> k) & 1u) apply_write(p, s.row[k], tx, pos, g.glane + k * G, s.readmask);
-    __threadfence();
+    fence_acq_rel();
 #pragma unroll
     for (int k = 0; k < K; ++k)
         if ((writes >> k) & 1u) atomicExch(p.meta + s.row[k], cts);
@@ -804,9 +865,9 @@ GCC_D int tictoc_read(const KParams &p, uint32_t row, uint32_t tx, uint64_t pos,
     }
     unsigned long long x1 = ld_cg(m);
     if (x1 & tictoc::kLock) return O_RETRY;
-    __threadfence();
+    fence_acq_rel();
     read_image(p, row_ptr(p, row), tx, pos, i, dt);
-    __threadfence();
+    fence_acq_rel();
     if (ld_cg(m) != x1) return O_RETRY;
     wts = tictoc::wts(x1);
     rts = tictoc::rts(x1);
@@ -864,6 +925,7 @@ GCC_D int attempt_tictoc(const KParams &p, const Group<G> &g, const TxOps<G> &s,
         if (ge) return kGiveUp;
         if (!gp) break;
         if (first) { first = false; cw = clock64(); }
+        wait_pause();
         if (g.any(expired(t0, p.spin_limit_ns) || error_raised(p.ctr))) {
             if (g.glane == 0) set_error(p.ctr, GCC_ETIMEOUT, W_TICTOC_READ);
             return kGiveUp;
@@ -893,20 +955,24 @@ GCC_D int attempt_tictoc(const KParams &p, const Group<G> &g, const TxOps<G> &s,
 #pragma unroll
         for (int k = 0; k < K; ++k)
             if ((held >> k) & 1u) atomicAnd(p.meta + s.row[k], ~tictoc::kLock);
-        __threadfence();
+        fence_acq_rel();
         return ge ? kGiveUp : kAbort;
     }
     // Serialization key: (batch, commit_ts, order of validation among equal
     // commit_ts). Within a batch commit_ts <= commits + 1 < 2^32.
-    if ((p.flags & GCC_F_COMMIT_LOG) && g.glane == 0) {
-        p.commit_hi[tx] = p.batch_st;
-        p.commit_lo[tx] = (cts << 32) | (atomicAdd(&p.ctr->seq, 1ull) & 0xFFFFFFFFull);
+    if (p.flags & GCC_F_COMMIT_LOG) {
+        g.sync();
+        if (g.glane == 0) {
+            p.commit_hi[tx] = p.batch_st;
+            p.commit_lo[tx] = (cts << 32) | (atomicAdd(&p.ctr->seq, 1ull) & 0xFFFFFFFFull);
+        }
+        g.sync();
     }
     if (p.write_mode == GCC_WRITE_ROWCOPY) g.sync();
 #pragma unroll
     for (int k = 0; k < K; ++k)
         if ((writes >> k) & 1u) apply_write(p, s.row[k], tx, pos, g.glane + k * G, s.readmask);
-    __threadfence();
+    fence_acq_rel();
 #pragma unroll
     for (int k = 0; k < K; ++k)
         if ((writes >> k) & 1u) atomicExch(p.meta + s.row[k], tictoc::make(false, 0, cts));
@@ -945,13 +1011,13 @@ GCC_D int attempt_ordered(const KParams &p, const Group<G> &g, const TxOps<G> &s
                 if (src >= 0 && !((done_ops >> src) & 1u)) continue;
             }
             if (ld_volatile(p.turn + s.row[k]) != mypos[k]) continue;
-            __threadfence();
+            fence_acq_rel();
             if (rd) {
                 read_image(p, row_ptr(p, s.row[k]), tx, pos, i, dg);
             } else {
                 apply_write(p, s.row[k], tx, pos, i, s.readmask);
             }
-            __threadfence();
+            fence_acq_rel();
             atomicExch(p.turn + s.row[k], mypos[k] + 1u);
             pending &= ~(1u << k);
             mine |= 1u << i;
@@ -960,6 +1026,7 @@ GCC_D int attempt_ordered(const KParams &p, const Group<G> &g, const TxOps<G> &s
         if (rowcopy) g.sync();
         if (!g.any(pending != 0u)) break;
         if (first) { first = false; cw = clock64(); }
+        wait_pause();
         if (g.any(expired(t0, p.spin_limit_ns) || error_raised(p.ctr))) {
             if (g.glane == 0) set_error(p.ctr, GCC_ETIMEOUT, W_TURN);
             return kGiveUp;
@@ -1070,6 +1137,15 @@ __global__ void __launch_bounds__(1024, 1) ycsb_kernel(const __grid_constant__ K
             st = attempt<SCH, G>(p, g, s, tx, pos, dg, ck, attempts > 0);
             if (st != kAbort) break;
             ++attempts;
+            // After 8 failed attempts, a short random pause (up to
+            // backoff_ns, at most a few microseconds) breaks the symmetric
+            // retry patterns that lock-step warps can otherwise repeat
+            // forever, e.g. two OCC transactions that each read what the
+            // other writes and abort on each other's write lock. It is kept
+            // short because a batch ends with its slowest transaction. The
+            // commit rule is untouched.
+            if (p.backoff_ns && attempts >= 8u)
+                __nanosleep((unsigned)(hash3(tx, attempts, 0x5ull) % p.backoff_ns));
             c_abort += clock64() - c_attempt;
             if (g.any(expired(t_start, 4ull * p.spin_limit_ns) || error_raised(p.ctr))) {
                 if (g.glane == 0) set_error(p.ctr, GCC_ETIMEOUT, W_RETRY);
@@ -1083,6 +1159,7 @@ __global__ void __launch_bounds__(1024, 1) ycsb_kernel(const __grid_constant__ K
             const long long c_end = clock64();
             p.digest[tx] = dg;
             p.tx_aborts[tx] = attempts;
+            if (attempts > 64) atomicMax(&p.ctr->max_attempts, attempts + 1u);
             atomicAdd(&s_met[0], 1ull);
             atomicAdd(&s_met[1], (unsigned long long)attempts);
             atomicAdd(&s_met[2], ck.ts);

@@ -544,6 +544,8 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
     p.flags = rp->flags;
     p.spin_limit_ns = rp->spin_limit_ns ? rp->spin_limit_ns : 4000000000ull;
     p.wait_die = (s == S_TPL_WD || s == S_SLOW_TPL_WD) ? 1u : 0u;
+    if (rp->backoff_ns < -1 || rp->backoff_ns > 100000) return GCC_EINVAL;
+    p.backoff_ns = rp->backoff_ns < 0 ? 0u : (rp->backoff_ns == 0 ? 512u : (uint32_t)rp->backoff_ns);
     p.scratch = rowcopy ? e->scratch : nullptr;
     p.read_log = want_log ? e->read_log : nullptr;
     p.ver_ts = e->ver_ts;
@@ -642,6 +644,8 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
     out->rank_count = gputx ? hc.max_rank + 1 : 0;
     out->batches = nbatches;
     out->kernel_launches = e->kernel_launches - launches0;
+    out->max_attempts = hc.max_attempts;
+    out->err_site = hc.err_where;
     // latency percentiles from the histogram (bucket upper edges)
     uint64_t total = 0;
     for (int i = 0; i < kHistBuckets; ++i) total += hc.hist[i];
@@ -664,6 +668,101 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
     if (hc.err) return (int)hc.err;
     if (hc.committed != e->n_tx) return GCC_ESTATE;
     return GCC_OK;
+}
+
+int gcc_run_checked(gcc_engine *e, const gcc_run_params *rp, gcc_result *out, int *verdict) {
+    if (!e || !rp || !out || !verdict) return GCC_EINVAL;
+    *verdict = 0;
+    if (!e->txs || e->n_tx == 0) return GCC_ESTATE;
+    cudaSetDevice(e->dev);
+    const size_t tbytes = e->rows * e->stride;
+    const uint64_t n = e->n_tx;
+    uint8_t *snap = nullptr, *final_t = nullptr;
+    unsigned long long *final_dg = nullptr, *diff = nullptr;
+    uint32_t *order_d = nullptr;
+    int rc = GCC_OK;
+    cudaError_t ce = cudaMalloc(&snap, tbytes);
+    if (ce == cudaSuccess) ce = cudaMalloc(&final_t, tbytes);
+    if (ce == cudaSuccess) ce = cudaMalloc(&final_dg, n * 8);
+    if (ce == cudaSuccess) ce = cudaMalloc(&diff, 8);
+    if (ce == cudaSuccess) ce = cudaMalloc(&order_d, n * 4);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(snap, e->table, tbytes, cudaMemcpyDeviceToDevice, e->stream);
+    gcc_run_params p = *rp;
+    p.flags |= GCC_F_COMMIT_LOG;
+    if (ce == cudaSuccess) {
+        rc = gcc_run(e, &p, out);
+        if (rc == GCC_OK) {
+            std::vector<gcc_commit_rec> log(n);
+            rc = gcc_get_commit_log(e, log.data(), n);
+            std::vector<uint32_t> order(n);
+            for (uint64_t i = 0; i < n; ++i) order[i] = (uint32_t)i;
+            std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+                if (log[a].hi != log[b].hi) return log[a].hi < log[b].hi;
+                if (log[a].lo != log[b].lo) return log[a].lo < log[b].lo;
+                return a < b;
+            });
+            cudaStream_t st = e->stream;
+            ce = cudaMemcpyAsync(final_t, e->table, tbytes, cudaMemcpyDeviceToDevice, st);
+            if (ce == cudaSuccess) ce = cudaMemcpyAsync(final_dg, e->digest, n * 8, cudaMemcpyDeviceToDevice, st);
+            if (ce == cudaSuccess) ce = cudaMemcpyAsync(order_d, order.data(), n * 4, cudaMemcpyHostToDevice, st);
+            if (ce == cudaSuccess) ce = cudaMemcpyAsync(e->table, snap, tbytes, cudaMemcpyDeviceToDevice, st);
+            if (ce == cudaSuccess) ce = cudaMemsetAsync(e->ctr, 0, sizeof(Counters), st);
+            // replay: one ordered launch over every transaction in log order
+            KParams q = e->base_params();
+            q.write_mode = rp->write_mode;
+            q.write_seed = rp->write_seed;
+            q.spin_limit_ns = rp->spin_limit_ns ? rp->spin_limit_ns : 4000000000ull;
+            q.order = order_d;
+            q.batch_st = 0;
+            q.batch_n = (uint32_t)n;
+            if (rp->write_mode == GCC_WRITE_ROWCOPY && e->scratch_units < n) {
+                rc = e->alloc(&e->scratch, n * kMaxOps * e->wslot * 8);
+                e->scratch_units = rc ? 0 : n;
+            }
+            q.scratch = rp->write_mode == GCC_WRITE_ROWCOPY ? e->scratch : nullptr;
+            if (ce == cudaSuccess && rc == GCC_OK) rc = e->order_pass(q, n, 0);
+            q.op_row = e->op_row;
+            q.op_pos = e->op_pos;
+            if (ce == cudaSuccess && rc == GCC_OK) {
+                const int block = 256;
+                int occ = scheme_occupancy(S_GACCO, 32, block);
+                int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((n * 32 + block - 1) / block,
+                                                                       (uint64_t)occ * e->sm_count));
+                k_batch_prep<<<1, 1, 0, st>>>(e->ctr, 0);
+                ce = launch_scheme_kernel(S_GACCO, 32, grid, block, q, st);
+            }
+            unsigned long long d_t = 0, d_d = 0;
+            if (ce == cudaSuccess) ce = cudaMemsetAsync(diff, 0, 8, st);
+            if (ce == cudaSuccess) {
+                k_count_diff<<<1024, 256, 0, st>>>((const unsigned long long *)final_t,
+                                                   (const unsigned long long *)e->table, tbytes / 8, diff);
+                ce = cudaMemcpyAsync(&d_t, diff, 8, cudaMemcpyDeviceToHost, st);
+            }
+            if (ce == cudaSuccess) ce = cudaMemsetAsync(diff, 0, 8, st);
+            if (ce == cudaSuccess) {
+                k_count_diff<<<256, 256, 0, st>>>(final_dg, e->digest, n, diff);
+                ce = cudaMemcpyAsync(&d_d, diff, 8, cudaMemcpyDeviceToHost, st);
+            }
+            unsigned err = 0;
+            if (ce == cudaSuccess) ce = cudaMemcpyAsync(&err, &e->ctr->err, 4, cudaMemcpyDeviceToHost, st);
+            if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+            if (ce == cudaSuccess && rc == GCC_OK) {
+                if (err) rc = (int)err;
+                *verdict = (!err && d_t == 0 && d_d == 0) ? 1 : 0;
+            }
+            // leave the engine in the checked run's final state
+            if (ce == cudaSuccess) ce = cudaMemcpyAsync(e->table, final_t, tbytes, cudaMemcpyDeviceToDevice, st);
+            if (ce == cudaSuccess) ce = cudaMemcpyAsync(e->digest, final_dg, n * 8, cudaMemcpyDeviceToDevice, st);
+            if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+        }
+    }
+    cudaFree(snap);
+    cudaFree(final_t);
+    cudaFree(final_dg);
+    cudaFree(diff);
+    cudaFree(order_d);
+    if (ce != cudaSuccess) return e->fail_cuda(ce);
+    return rc;
 }
 
 int gcc_format_line(const gcc_run_params *p, const gcc_result *r, char *buf, size_t n) {

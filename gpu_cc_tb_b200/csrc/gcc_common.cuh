@@ -101,6 +101,7 @@ struct Counters {
     unsigned long long max_rank;   // gputx
     unsigned int err;              // first error status (negative gcc code)
     unsigned int err_where;        // diagnostic: which wait gave up
+    unsigned int max_attempts;     // most attempts of one transaction
     unsigned int hist[kHistBuckets];
 };
 
@@ -161,6 +162,7 @@ struct KParams {
     uint64_t spin_limit_ns;
     uint32_t flags;
     uint32_t wait_die;
+    uint32_t backoff_ns;        // 0: retry at once
 };
 
 // ---------------------------------------------------------------------------
@@ -181,6 +183,12 @@ GCC_D unsigned long long ld_volatile(const unsigned long long *p) {
 GCC_D unsigned int ld_volatile(const unsigned int *p) {
     return *(const volatile unsigned int *)p;
 }
+// Acquire/release fence at GPU scope: orders this thread's earlier memory
+// operations before its later ones, which is all the lock/timestamp
+// protocols here need (no store->load Dekker patterns), and is cheaper than
+// the sequentially consistent fence behind __threadfence().
+GCC_D void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
 GCC_D void set_error(Counters *c, int code, unsigned where) {
     if (atomicCAS(&c->err, 0u, (unsigned)code) == 0u) c->err_where = where;
 }

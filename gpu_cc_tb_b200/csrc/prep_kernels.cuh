@@ -300,6 +300,15 @@ __global__ void k_iota(uint32_t *v, uint64_t n) {
     if (i < n) v[i] = (uint32_t)i;
 }
 
+// Count differing 8-byte words of two buffers (replay check).
+__global__ void k_count_diff(const unsigned long long *a, const unsigned long long *b, uint64_t n,
+                             unsigned long long *diff) {
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    unsigned long long d = 0;
+    for (; i < n; i += (uint64_t)gridDim.x * blockDim.x) d += a[i] != b[i];
+    if (d) atomicAdd(diff, d);
+}
+
 // Per-launch counter reset: ticket = 0 and, for TO/MVCC, ts = 1
 // (NaiveTSAllocator_CPU::Init, include/timestamp.cuh:76-80).
 __global__ void k_batch_prep(Counters *c, int reset_ts) {

@@ -110,7 +110,12 @@ typedef struct gcc_run_params {
     int32_t batch_size;    /* transactions per batch (gputx ranks all) */
     uint32_t flags;        /* GCC_F_* */
     int32_t write_mode;    /* GCC_WRITE_* */
-    int32_t reserved;
+    int32_t backoff_ns;    /* retry pause: after 8 failed attempts each retry
+                              first sleeps a random 0..backoff_ns ns (0 means
+                              512); -1 never sleeps (the reference retries at
+                              once, benchmark/ycsb.cu:101, which lets two OCC
+                              transactions with crossing read/write sets abort
+                              each other indefinitely) */
     uint64_t write_seed;   /* seed of GCC_WRITE_FIELD values */
     uint64_t spin_limit_ns;/* bound of any single device wait; 0 = 4 s */
 } gcc_run_params;
@@ -128,6 +133,8 @@ typedef struct gcc_result {
     uint64_t rank_count;           /* gputx: number of ranks */
     uint64_t batches;              /* kernel batches launched */
     uint64_t kernel_launches;      /* engine kernels launched by the run */
+    uint32_t max_attempts;         /* most attempts any one tx needed */
+    uint32_t err_site;             /* where a bounded wait gave up (0: none) */
 } gcc_result;
 
 /* Serialization key of one committed transaction: replaying transactions in
@@ -165,6 +172,15 @@ int gcc_load_txs(gcc_engine *e, const gcc_ycsb_tx *txs, uint64_t n_tx);
 /* Execute every loaded transaction under one scheme (the batch loop of
  * benchmark_cpu/ycsb.cu:249-292). Synchronous. */
 int gcc_run(gcc_engine *e, const gcc_run_params *p, gcc_result *out);
+
+/* gcc_run plus a serializability check (the role of ExecInfo::Check,
+ * src/runtime.cu:129-158, run on the GPU): the committed transactions are
+ * executed again, one after another in their recorded serialization order,
+ * from the table as it was before the run, by the deterministic ordered
+ * executor; *verdict = 1 when that reproduces the run's final table and
+ * every read digest, else 0. The engine is left in the run's final state. */
+int gcc_run_checked(gcc_engine *e, const gcc_run_params *p, gcc_result *out,
+                    int *verdict);
 
 /* Reference output line (ExecInfo::Analyse CSV columns) for a result. */
 int gcc_format_line(const gcc_run_params *p, const gcc_result *r, char *buf,

@@ -23,7 +23,7 @@ def declared_symbols():
 
 def test_library_exports_every_declared_symbol(gcc):
     syms = declared_symbols()
-    assert len(syms) >= 19
+    assert len(syms) >= 20
     out = subprocess.run(["nm", "-D", "--defined-only", str(g.library_path())],
                          capture_output=True, text=True, check=True).stdout
     exported = set(re.findall(r"\bT (gcc_[a-z_0-9]+)", out))
@@ -95,7 +95,7 @@ def test_generator_rejects_bad_arguments(gcc):
 
 def test_result_line_format(gcc):
     lib = g.library()
-    p = g.RunParams(b"tpl_nw", 5, 32, 65536, 0, 0, 0, 1, 0)
+    p = g.RunParams(b"tpl_nw", 5, 32, 65536, 0, 0, 0, 1, 0)  # backoff 0, seed 1
     r = g.Result()
     r.tx_per_s, r.aborts, r.tot_s, r.pre_s, r.proc_s = 18670000.0, 15736673, 0.0561, 0.001, 0.05
     r.ts_d, r.wait_d, r.abort_d, r.mng_d, r.tot_d, r.idx_d = 0, 1e-4, 0.5, 0.25, 0.183, 0.085
