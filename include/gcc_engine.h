@@ -198,6 +198,28 @@ int gcc_get_read_log(gcc_engine *e, void *dst, uint64_t bytes);
 int gcc_index_lookup(gcc_engine *e, const uint32_t *keys, uint32_t *rows,
                      uint64_t n);
 
+/* 2PL no-wait over caller-owned device buffers, allocating no device memory
+ * (no counterpart in the reference). For callers that cannot call cudaMalloc:
+ * code whose device memory belongs to another allocator (a framework's pool,
+ * a pre-sized arena) or that runs on a latency-bound thread where
+ * cudaMalloc's implicit device synchronisation is not acceptable. All
+ * pointers are device pointers owned by the caller: `txs` (n_tx gen_ycsb
+ * records, keys are row ids), `table` (rows x 96-byte rows of the u64x11
+ * layout, updated in place), outputs `digests` (n_tx) and `tx_aborts`
+ * (n_tx). Writes are GCC_WRITE_FIELD with `write_seed`. Scratch (a lock word
+ * per row and the run counters) lives in a static device array of this
+ * library: at most 1,048,576 rows (8 MiB), held by every GPU that loads the
+ * library until exit; larger tables are rejected with GCC_EINVAL. Calls on a
+ * device share that array and clear it before use, so calls that overlap on
+ * the GPU race. The first call on a device looks up the array's address with
+ * the device current; make it before any stream capture. Runs on `stream`
+ * (a cudaStream_t, may be null) and waits for it; committed / aborts may be
+ * null. */
+int gcc_run_tpl_nw_noalloc(const gcc_ycsb_tx *txs, uint64_t n_tx, void *table,
+                           uint64_t rows, uint64_t *digests, uint32_t *tx_aborts,
+                           uint64_t write_seed, void *stream, uint64_t *committed,
+                           uint64_t *aborts);
+
 /* Device-side timing of the last run's main kernels: total ms and number of
  * launches of the transaction kernel (for roofline accounting). */
 int gcc_last_kernel_ms(gcc_engine *e, double *kernel_ms, uint64_t *launches);
