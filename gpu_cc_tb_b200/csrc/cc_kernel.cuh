@@ -34,6 +34,7 @@ namespace gcc {
 
 namespace cg = cooperative_groups;
 
+
 enum Scheme : int {
     S_TPL_NW = 0, S_TPL_WD, S_TO, S_MVCC, S_SILO, S_TICTOC, S_GACCO, S_GPUTX,
     S_SLOW_TPL_NW, S_SLOW_TPL_WD, S_SLOW_TO, S_SLOW_MVCC, S_SLOW_SILO,
@@ -163,6 +164,27 @@ GCC_D void apply_write(const KParams &p, uint32_t row, uint32_t tx, uint64_t pos
 }
 
 // ---------------------------------------------------------------------------
+// Retry timing: after an aborted attempt has released everything it held,
+// the lane whose request failed polls that row's word (plain loads, short
+// sleeps) until it looks compatible, at most kObstacleWaitNs, so the retry
+// is not spent against the same conflict. The lock requests themselves keep
+// the scheme's rule (e.g. no-wait: a conflicting request aborts).
+// ---------------------------------------------------------------------------
+constexpr uint64_t kObstacleWaitNs = 50000;
+// want_zero: wait for the word to be 0; otherwise wait until (word & mask) == 0
+GCC_D void await_row(const KParams &p, uint32_t row, unsigned long long mask, bool want_zero) {
+    if (row == kNoRow || (p.flags & GCC_F_RETRY_IMMEDIATE)) return;
+    const uint64_t t0 = gtimer();
+    const uint64_t lim = p.spin_limit_ns < kObstacleWaitNs ? p.spin_limit_ns : kObstacleWaitNs;
+    while (true) {
+        unsigned long long w = ld_cg(p.meta + row);
+        if (want_zero ? w == 0ull : (w & mask) == 0ull) return;
+        if (gtimer() - t0 > lim) return;
+        __nanosleep(64);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Latches of the slow_* variants (runtime.cuh:91-109), bounded.
 // ---------------------------------------------------------------------------
 GCC_D bool latch_acquire(const KParams &p, uint32_t row) {
@@ -213,7 +235,7 @@ GCC_D int tpl_shared(const KParams &p, uint32_t row, uint32_t tx) {
         unsigned long long w = ld_cg(m);
         if (w & tpl::kExcl) return tpl::holder(w) < tx ? L_DIE : L_WAIT;
     }
-    unsigned long long old = atomicAdd(m, 1ull);
+    unsigned long long old = atom_add_acq(m, 1ull);
     if (!(old & tpl::kExcl)) return L_OK;
     atomicAdd(m, ~0ull);  // undo the speculative reader increment
     if (!WD) return L_DIE;
@@ -221,7 +243,7 @@ GCC_D int tpl_shared(const KParams &p, uint32_t row, uint32_t tx) {
 }
 template <bool WD>
 GCC_D int tpl_excl(const KParams &p, uint32_t row, uint32_t tx) {
-    unsigned long long old = atomicCAS(p.meta + row, 0ull, tpl::excl_word(tx));
+    unsigned long long old = atom_cas_acq(p.meta + row, 0ull, tpl::excl_word(tx));
     if (old == 0ull) return L_OK;
     if (!WD) return L_DIE;
     if (!(old & tpl::kExcl)) return L_DIE;  // shared holders: requester dies
@@ -248,8 +270,9 @@ GCC_D int slow_tpl_lock(const KParams &p, uint32_t row, uint32_t tx, bool shared
 template <bool SLOW>
 GCC_D bool tpl_unlock(const KParams &p, uint32_t row, bool shared) {
     if (!SLOW) {
-        if (shared) atomicAdd(p.meta + row, ~0ull);
-        else atomicAnd(p.meta + row, tpl::kReaders);
+        // release: this lane's reads / writes of the row come before
+        if (shared) red_add_rel(p.meta + row, ~0ull);
+        else red_and_rel(p.meta + row, tpl::kReaders);
         return true;
     }
     if (shared) {
@@ -283,6 +306,8 @@ GCC_D int attempt_tpl(const KParams &p, const Group<G> &g, const TxOps<G> &s, ui
     constexpr int K = TxOps<G>::K;
     uint32_t held = 0, pending = s.valid;
     bool fail = false, err = false;
+    uint32_t obst = kNoRow;  // row whose lock request failed
+    bool obst_x = false;     // ... and whether it was an exclusive request
     uint64_t t0 = gtimer();
     long long cw = clock64();
     bool first = true;
@@ -306,6 +331,7 @@ GCC_D int attempt_tpl(const KParams &p, const Group<G> &g, const TxOps<G> &s, ui
                         }
                     }
                     if (r == L_OK) held |= 1u << k;
+                    else if (r == L_DIE) { obst = s.row[k]; obst_x = !((s.isread >> k) & 1u); }
                 }
             }
             r = g.bcast(r, owner);
@@ -319,7 +345,11 @@ GCC_D int attempt_tpl(const KParams &p, const Group<G> &g, const TxOps<G> &s, ui
                 if (!((pending >> k) & 1u) || fail || err) continue;
                 int r = tpl_lock<WD, SLOW>(p, s.row[k], tx, (s.isread >> k) & 1u);
                 if (r == L_OK) { held |= 1u << k; pending &= ~(1u << k); }
-                else if (r == L_DIE) fail = true;
+                else if (r == L_DIE) {
+                    fail = true;
+                    obst = s.row[k];
+                    obst_x = !((s.isread >> k) & 1u);
+                }
                 else if (r == L_ERR) err = true;
             }
             bool gf = g.any(fail), ge = g.any(err), gp = g.any(pending != 0u);
@@ -338,9 +368,14 @@ GCC_D int attempt_tpl(const KParams &p, const Group<G> &g, const TxOps<G> &s, ui
 #pragma unroll
         for (int k = 0; k < K; ++k)
             if ((held >> k) & 1u) tpl_unlock<SLOW>(p, s.row[k], (s.isread >> k) & 1u);
-        return err ? kGiveUp : kAbort;
+        if (err) return kGiveUp;
+        // an exclusive request waits for a free word, a shared one for the
+        // exclusive holder to leave
+        await_row(p, obst, tpl::kExcl, obst_x);
+        return kAbort;
     }
-    fence_acq_rel();
+    // (the fast variants' lock RMWs are acquire operations)
+    if (SLOW) fence_acq_rel();
     // Serialization point: every lock is held. The leader's sequence number
     // is ordered after every lane's acquisition and before every lane's
     // release by the two warp syncs (lanes' memory operations are otherwise
@@ -364,7 +399,8 @@ GCC_D int attempt_tpl(const KParams &p, const Group<G> &g, const TxOps<G> &s, ui
     for (int k = 0; k < K; ++k)
         if (((s.valid & ~s.isread) >> k) & 1u)
             apply_write(p, s.row[k], tx, pos, (uint32_t)(g.glane + k * G), s.readmask);
-    fence_acq_rel();
+    // (the fast variants' unlocks are release operations)
+    if (SLOW) fence_acq_rel();
     bool uerr = false;
 #pragma unroll
     for (int k = 0; k < K; ++k)
@@ -728,7 +764,7 @@ GCC_D int occ_lock(const KParams &p, uint32_t row, unsigned long long lockbit,
 template <int G, bool SLOW, bool TICTOC>
 GCC_D void occ_lock_writes(const KParams &p, const Group<G> &g, const TxOps<G> &s,
                            uint32_t writes, bool ordered, uint32_t &held,
-                           unsigned long long &cts, bool &fail, bool &err) {
+                           unsigned long long &cts, bool &fail, bool &err, uint32_t &obst) {
     constexpr int K = TxOps<G>::K;
     const unsigned long long lockbit = TICTOC ? tictoc::kLock : silo::kLock;
     if (!ordered) {
@@ -741,7 +777,7 @@ GCC_D void occ_lock_writes(const KParams &p, const Group<G> &g, const TxOps<G> &
                 held |= 1u << k;
                 unsigned long long c = TICTOC ? tictoc::rts(cur) + 1ull : silo::ts(cur);
                 cts = cts > c ? cts : c;
-            } else if (r == O_FAIL) fail = true;
+            } else if (r == O_FAIL) { fail = true; obst = s.row[k]; }
             else err = true;
         }
         return;
@@ -759,7 +795,7 @@ GCC_D void occ_lock_writes(const KParams &p, const Group<G> &g, const TxOps<G> &
                     held |= 1u << k;
                     unsigned long long c = TICTOC ? tictoc::rts(cur) + 1ull : silo::ts(cur);
                     cts = cts > c ? cts : c;
-                }
+                } else if (r == O_FAIL) obst = s.row[k];
             }
         }
         r = g.bcast(r, owner);
@@ -802,7 +838,8 @@ GCC_D int attempt_silo(const KParams &p, const Group<G> &g, const TxOps<G> &s, u
     if (!first) ck.wait += clock64() - cw;
     // validation: lock the write set, no-wait (silo.cuh:268-281)
     unsigned long long cts = 0;
-    occ_lock_writes<G, SLOW, false>(p, g, s, writes, ordered, held, cts, fail, err);
+    uint32_t obst = kNoRow;
+    occ_lock_writes<G, SLOW, false>(p, g, s, writes, ordered, held, cts, fail, err, obst);
     bool gf = g.any(fail), ge = g.any(err);
     if (!gf && !ge) {
         fence_acq_rel();
@@ -821,7 +858,10 @@ GCC_D int attempt_silo(const KParams &p, const Group<G> &g, const TxOps<G> &s, u
         for (int k = 0; k < K; ++k) {
             if (!((reads >> k) & 1u)) continue;
             unsigned long long x = ld_cg(p.meta + s.row[k]);
-            if (silo::ts(x) != rec[k] || (x & silo::kLock)) fail = true;
+            if (silo::ts(x) != rec[k] || (x & silo::kLock)) {
+                fail = true;
+                if (x & silo::kLock) obst = s.row[k];
+            }
             cts = cts > rec[k] ? cts : rec[k];
         }
         gf = g.any(fail);
@@ -933,7 +973,8 @@ GCC_D int attempt_tictoc(const KParams &p, const Group<G> &g, const TxOps<G> &s,
     }
     if (!first) ck.wait += clock64() - cw;
     unsigned long long cts = 0;
-    occ_lock_writes<G, SLOW, true>(p, g, s, writes, ordered, held, cts, fail, err);
+    uint32_t obst = kNoRow;
+    occ_lock_writes<G, SLOW, true>(p, g, s, writes, ordered, held, cts, fail, err, obst);
     bool gf = g.any(fail), ge = g.any(err);
     if (!gf && !ge) {
 #pragma unroll
@@ -945,7 +986,7 @@ GCC_D int attempt_tictoc(const KParams &p, const Group<G> &g, const TxOps<G> &s,
             if (!((reads >> k) & 1u) || fail || err) continue;
             if (rr[k] >= cts) continue;
             int r = tictoc_extend<SLOW>(p, s.row[k], rw[k], cts);
-            if (r == O_FAIL) fail = true;
+            if (r == O_FAIL) { fail = true; obst = s.row[k]; }
             else if (r == O_ERR) err = true;
         }
         gf = g.any(fail);
@@ -1010,15 +1051,15 @@ GCC_D int attempt_ordered(const KParams &p, const Group<G> &g, const TxOps<G> &s
                 int src = rowcopy_src(s.readmask, i);
                 if (src >= 0 && !((done_ops >> src) & 1u)) continue;
             }
-            if (ld_volatile(p.turn + s.row[k]) != mypos[k]) continue;
-            fence_acq_rel();
+            // acquire: the predecessor's access to the row is visible
+            if (ld_acquire(p.turn + s.row[k]) != mypos[k]) continue;
             if (rd) {
                 read_image(p, row_ptr(p, s.row[k]), tx, pos, i, dg);
             } else {
                 apply_write(p, s.row[k], tx, pos, i, s.readmask);
             }
-            fence_acq_rel();
-            atomicExch(p.turn + s.row[k], mypos[k] + 1u);
+            // release: this access comes before the successor's
+            st_release(p.turn + s.row[k], mypos[k] + 1u);
             pending &= ~(1u << k);
             mine |= 1u << i;
         }
@@ -1076,12 +1117,29 @@ __global__ void __launch_bounds__(1024, 1) ycsb_kernel(const __grid_constant__ K
     const Group<G> g;
     constexpr int K = TxOps<G>::K;
 
+    // Positions come from 32 striped ticket counters (stripe j hands out
+    // j, j + 32, j + 64, ... in increasing order, each counter on its own
+    // 128-byte line): one same-address atomic per transaction on a single
+    // counter was the main latency term at low contention. A group starts on
+    // stripe (group id % 32) and moves to the next stripe when its stripe is
+    // exhausted. Within a stripe positions are taken in order and a group
+    // runs one position at a time, so the lowest unfinished position is
+    // always held by a running group (the ordered schemes' hand-off stays
+    // live).
+    const unsigned gid = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    unsigned stripe = gid % kTicketStripes, tried = 0;
     while (true) {
         unsigned long long pos = 0;
         unsigned stop = 0;
         if (g.glane == 0) {
-            pos = atomicAdd(&p.ctr->ticket, 1ull);
-            stop = (pos >= p.batch_n || error_raised(p.ctr)) ? 1u : 0u;
+            while (true) {
+                unsigned long long t = atomicAdd(&p.ctr->tickets[stripe * 16], 1ull);
+                pos = t * kTicketStripes + stripe;
+                if (pos < p.batch_n) break;
+                if (++tried >= kTicketStripes) { stop = 1u; break; }
+                stripe = (stripe + 1) % kTicketStripes;
+            }
+            if (error_raised(p.ctr)) stop = 1u;
         }
         stop = g.bcast(stop, 0);
         if (stop) break;

@@ -585,7 +585,7 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
                            s == S_SLOW_TICTOC);
         if (!ordered && !(keep && b > 0)) CKR(cudaMemsetAsync(e->meta, 0, e->rows * 8, st));
         if (is_mvcc(s)) CKR(cudaMemsetAsync(e->turn, 0xFF, e->rows * 4, st));
-        k_batch_prep<<<1, 1, 0, st>>>(e->ctr, uses_ts(s) ? 1 : 0);
+        k_batch_prep<<<1, 32, 0, st>>>(e->ctr, uses_ts(s) ? 1 : 0);
         CKR(cudaGetLastError());
         e->kernel_launches += 1;
         if (s == S_GACCO) {
@@ -728,7 +728,7 @@ int gcc_run_checked(gcc_engine *e, const gcc_run_params *rp, gcc_result *out, in
                 int occ = scheme_occupancy(S_GACCO, 32, block);
                 int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((n * 32 + block - 1) / block,
                                                                        (uint64_t)occ * e->sm_count));
-                k_batch_prep<<<1, 1, 0, st>>>(e->ctr, 0);
+                k_batch_prep<<<1, 32, 0, st>>>(e->ctr, 0);
                 ce = launch_scheme_kernel(S_GACCO, 32, grid, block, q, st);
             }
             unsigned long long d_t = 0, d_d = 0;

@@ -89,9 +89,11 @@ GCC_HD uint64_t make(bool lock, uint64_t delta, uint64_t wts) {
 // Run-wide counters, metrics and latency histogram (device memory).
 // ---------------------------------------------------------------------------
 constexpr int kHistBuckets = 1024;  // 64 octaves x 16 linear sub-buckets (ns)
+constexpr int kTicketStripes = 32;  // ticket counters, one per 128-byte line
 
 struct Counters {
-    unsigned long long ticket;     // next position in the execution order
+    // stripe j hands out positions j, j + 32, j + 64, ... in order
+    unsigned long long tickets[kTicketStripes * 16];
     unsigned long long seq;        // serialization sequence (commit log)
     unsigned long long ts;         // timestamp allocator (TO, MVCC)
     unsigned long long committed;  // committed transactions
@@ -188,6 +190,37 @@ GCC_D unsigned int ld_volatile(const unsigned int *p) {
 // protocols here need (no store->load Dekker patterns), and is cheaper than
 // the sequentially consistent fence behind __threadfence().
 GCC_D void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+// Atomics with acquire / release semantics at GPU scope: the lock RMW orders
+// this lane's later accesses to the row after it (acquire) and the unlock
+// RMW orders its earlier accesses before it (release), without a standalone
+// fence.
+GCC_D unsigned long long atom_add_acq(unsigned long long *p, unsigned long long v) {
+    unsigned long long r;
+    asm volatile("atom.acquire.gpu.global.add.u64 %0, [%1], %2;" : "=l"(r) : "l"(p), "l"(v) : "memory");
+    return r;
+}
+GCC_D unsigned long long atom_cas_acq(unsigned long long *p, unsigned long long cmp,
+                                      unsigned long long val) {
+    unsigned long long r;
+    asm volatile("atom.acquire.gpu.global.cas.b64 %0, [%1], %2, %3;"
+                 : "=l"(r) : "l"(p), "l"(cmp), "l"(val) : "memory");
+    return r;
+}
+GCC_D void red_add_rel(unsigned long long *p, unsigned long long v) {
+    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
+}
+GCC_D void red_and_rel(unsigned long long *p, unsigned long long v) {
+    asm volatile("red.release.gpu.global.and.b64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
+}
+GCC_D unsigned ld_acquire(const unsigned *p) {
+    unsigned r;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(r) : "l"(p) : "memory");
+    return r;
+}
+GCC_D void st_release(unsigned *p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
+}
 
 GCC_D void set_error(Counters *c, int code, unsigned where) {
     if (atomicCAS(&c->err, 0u, (unsigned)code) == 0u) c->err_where = where;

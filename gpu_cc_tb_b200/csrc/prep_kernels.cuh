@@ -309,11 +309,11 @@ __global__ void k_count_diff(const unsigned long long *a, const unsigned long lo
     if (d) atomicAdd(diff, d);
 }
 
-// Per-launch counter reset: ticket = 0 and, for TO/MVCC, ts = 1
+// Per-launch counter reset: ticket stripes = 0 and, for TO/MVCC, ts = 1
 // (NaiveTSAllocator_CPU::Init, include/timestamp.cuh:76-80).
 __global__ void k_batch_prep(Counters *c, int reset_ts) {
-    c->ticket = 0ull;
-    if (reset_ts) c->ts = 1ull;
+    if (threadIdx.x < kTicketStripes) c->tickets[threadIdx.x * 16] = 0ull;
+    if (threadIdx.x == 0 && reset_ts) c->ts = 1ull;
 }
 
 }  // namespace gcc

@@ -72,6 +72,9 @@ extern "C" {
 #define GCC_F_READ_LOG 2u   /* record every read row image (parity runs) */
 #define GCC_F_NO_RESET 4u   /* keep CC metadata across batches where the
                                scheme allows it (tpl, silo, tictoc) */
+#define GCC_F_RETRY_IMMEDIATE 8u /* retry an aborted transaction at once
+                               instead of first waiting (up to 50 us) until
+                               the row that made it abort looks free */
 
 /* Dataset generator dedup modes (gen_ycsb drops repeated keys, which leaves
  * fewer than 16 requests; resample redraws until 16 distinct keys). */

@@ -58,8 +58,8 @@ def run_and_check(oracle, eng, init, txs, scheme, wd, bs, batch, write_mode, lay
 
 @pytest.fixture(scope="module")
 def small_u64(oracle):
-    rows, layout = 16384, g.LAYOUT_U64X11
-    txs = g.gen_ycsb(rows, 8192, 0.7, 0.8, seed=11, dedup=g.DEDUP_RESAMPLE, key_base=0)
+    rows, layout = 65536, g.LAYOUT_U64X11
+    txs = g.gen_ycsb(rows, 8192, 0.6, 0.8, seed=11, dedup=g.DEDUP_RESAMPLE, key_base=0)
     init = oracle.fill_table(rows, layout, 141919810)
     eng = g.Engine(rows, layout=layout, index=g.INDEX_HASH, fill_seed=141919810, max_batch=2048)
     eng.load_txs(txs)
