@@ -140,44 +140,6 @@ def algorithmic_bytes(txs, row_bytes=88, write_bytes=8):
     return 8 * len(txs) + 8 * ops + reads * (32 + row_bytes) + writes * (32 + write_bytes), reads, writes
 
 
-def dist_init():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    if ws <= 1:
-        return 0, 1, 0, None
-    import torch
-    import torch.distributed as dist
-    from datetime import timedelta
-    rank, local = int(os.environ["RANK"]), int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    return rank, ws, local, dist
-
-
-def reduce_max(dist, v, local):
-    if dist is None:
-        return v
-    import torch
-    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def reduce_sum(dist, v, local):
-    if dist is None:
-        return v
-    import torch
-    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
-
-
-def barrier(dist, local):
-    import torch
-    if dist is not None:
-        dist.barrier()
-    torch.cuda.synchronize(local)
-
-
 def config_of(a):
     return {
         "workload": f"ycsb_plain_{a.rows}rows_{a.txs}tx_16ops_theta{a.theta}_r{a.read_ratio}",
@@ -246,7 +208,8 @@ def main():
     if a.impl == "reference":
         run_reference(a)
         return
-    rank, ws, local, dist = dist_init()
+    from gpu_cc_tb_b200 import replicas
+    rank, ws, local, dist = replicas.init_from_env("nccl")
     import torch
     import gpu_cc_tb_b200 as g
     index = {"hash": g.INDEX_HASH, "sorted": g.INDEX_SORTED, "direct": g.INDEX_DIRECT}[a.index]
@@ -269,7 +232,7 @@ def main():
         eng.run(a.scheme, **kw)
 
     clocks = Clocks(local)
-    barrier(dist, local)
+    replicas.barrier(dist)
     clocks.start()
     dev_s, kern_ms, launches, committed, aborts = 0.0, 0.0, 0, 0, 0
     lat50, lat99 = [], []
@@ -286,25 +249,22 @@ def main():
         lat99.append(r["lat_p99_us"])
         n_tx_launches = r["batches"]
     wall = time.perf_counter() - t0
-    barrier(dist, local)
+    replicas.barrier(dist)
     clk = clocks.stop()
 
     # end to end through the public API: H2D of the step's transactions from
     # pinned memory, the run, D2H of every transaction's read digest
     e2e_s = 0.0
     for _ in range(a.steps):
-        barrier(dist, local)
+        replicas.barrier(dist)
         s0 = time.perf_counter()
         eng.load_txs(host_txs)
         eng.run(a.scheme, **kw)
         g.library().gcc_get_digests(eng._h, g.C.c_void_p(digests_host.ctypes.data), a.txs)
         e2e_s += time.perf_counter() - s0
 
-    dev_s_max = reduce_max(dist, dev_s, local)
-    e2e_max = reduce_max(dist, e2e_s, local)
-    total_committed = reduce_sum(dist, committed, local)
-    value = total_committed / dev_s_max
-    e2e_val = reduce_sum(dist, a.steps * a.txs, local) / e2e_max
+    job = replicas.combine(dist, dev_s, committed, e2e_s, a.steps * a.txs)
+    dev_s_max, value, e2e_val = job["device_s_max"], job["value"], job["e2e_value"]
 
     if rank == 0:
         hbm, kind = peaks()
