@@ -23,6 +23,8 @@ __all__ = [
     "INDEX_DIRECT", "WRITE_FIELD", "WRITE_ROWCOPY", "F_COMMIT_LOG", "F_READ_LOG",
     "F_NO_RESET", "DEDUP_DROP", "DEDUP_RESAMPLE", "TX_DTYPE", "GccError", "Engine",
     "gen_ycsb", "library", "library_path", "scheme_id", "row_bytes", "row_stride",
+    "gen_ycsb_var", "REQ_DTYPE", "F_RETRY_IMMEDIATE", "F_AUTOTUNE", "F_GRAPH",
+    "BATCHES_SEQUENTIAL", "BATCHES_QUEUE", "VAR_SCHEMES",
 ]
 
 PKG = Path(__file__).resolve().parent
@@ -35,7 +37,9 @@ SCHEMES = ("tpl_nw", "tpl_wd", "to", "mvcc", "silo", "tictoc", "gacco", "gputx",
 LAYOUT_U64X11, LAYOUT_REF104 = 0, 1
 INDEX_HASH, INDEX_SORTED, INDEX_DIRECT = 0, 1, 2
 WRITE_FIELD, WRITE_ROWCOPY = 0, 1
-F_COMMIT_LOG, F_READ_LOG, F_NO_RESET = 1, 2, 4
+F_COMMIT_LOG, F_READ_LOG, F_NO_RESET, F_RETRY_IMMEDIATE = 1, 2, 4, 8
+F_AUTOTUNE, F_GRAPH = 16, 32
+BATCHES_SEQUENTIAL, BATCHES_QUEUE = 0, 1
 DEDUP_DROP, DEDUP_RESAMPLE = 0, 1
 
 STATUS = {0: "GCC_OK", -1: "GCC_EINVAL", -2: "GCC_ENOMEM", -3: "GCC_ECUDA", -4: "GCC_ETIMEOUT",
@@ -46,6 +50,9 @@ STATUS = {0: "GCC_OK", -1: "GCC_EINVAL", -2: "GCC_ENOMEM", -3: "GCC_ECUDA", -4: 
 TX_DTYPE = np.dtype([("request_cnt", "<u8"),
                      ("requests", np.dtype([("read", "<i4"), ("key", "<u4")]), (16,))])
 assert TX_DTYPE.itemsize == 136
+REQ_DTYPE = np.dtype([("read", "<i4"), ("key", "<u4")])
+# schemes of the batched executors (gcc_run_batches); mvcc: sequential only
+VAR_SCHEMES = ("tpl_nw", "tpl_wd", "to", "silo", "tictoc", "mvcc")
 
 
 class GccError(RuntimeError):
@@ -127,6 +134,13 @@ def library() -> C.CDLL:
         "gcc_get_read_log": (C.c_int, [P, P, C.c_uint64]),
         "gcc_index_lookup": (C.c_int, [P, P, P, C.c_uint64]),
         "gcc_last_kernel_ms": (C.c_int, [P, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
+        "gcc_gen_ycsb_var_offsets": (C.c_int, [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, P]),
+        "gcc_gen_ycsb_var": (C.c_int, [C.c_uint64, C.c_uint64, C.c_double, C.c_double,
+                                       C.c_uint64, C.c_int32, C.c_int32, P, P]),
+        "gcc_load_var_txs": (C.c_int, [P, P, P, C.c_uint64]),
+        "gcc_run_batches": (C.c_int, [P, C.POINTER(RunParams), P, C.c_uint64, C.c_int32,
+                                      C.POINTER(Result)]),
+        "gcc_get_batch_stats": (C.c_int, [P, P, P, P, C.c_uint64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -166,6 +180,19 @@ def gen_ycsb(rows: int, n_tx: int, theta: float, read_ratio: float, seed: int = 
     _check(library().gcc_gen_ycsb(rows, n_tx, theta, read_ratio, seed, dedup, key_base, threads,
                                   _ptr(out)), "gcc_gen_ycsb")
     return out
+
+
+def gen_ycsb_var(rows: int, n_tx: int, theta: float, read_ratio: float, min_ops: int = 4,
+                 max_ops: int = 64, seed: int = 141919810, key_base: int = 0, threads: int = 0):
+    """Variable-length transactions: (tx_off[n_tx + 1] uint32, reqs REQ_DTYPE)."""
+    lib = library()
+    off = np.zeros(n_tx + 1, dtype=np.uint32)
+    _check(lib.gcc_gen_ycsb_var_offsets(n_tx, min_ops, max_ops, seed, _ptr(off)),
+           "gcc_gen_ycsb_var_offsets")
+    reqs = np.zeros(int(off[-1]), dtype=REQ_DTYPE)
+    _check(lib.gcc_gen_ycsb_var(rows, n_tx, theta, read_ratio, seed, key_base, threads,
+                                _ptr(off), _ptr(reqs)), "gcc_gen_ycsb_var")
+    return off, reqs
 
 
 class Engine:
@@ -234,6 +261,35 @@ class Engine:
         self.last_result = r.as_dict()
         _check(rc, f"gcc_run_checked({scheme})")
         return r.as_dict(), v.value == 1
+
+    def load_var_txs(self, tx_off: np.ndarray, reqs: np.ndarray):
+        tx_off = np.ascontiguousarray(tx_off, dtype=np.uint32)
+        reqs = np.ascontiguousarray(reqs, dtype=REQ_DTYPE)
+        _check(self.lib.gcc_load_var_txs(self._h, _ptr(tx_off), _ptr(reqs), len(tx_off) - 1),
+               "gcc_load_var_txs")
+        self.n_var = len(tx_off) - 1
+
+    def run_batches(self, scheme: str, batch_off, mode: int = BATCHES_SEQUENTIAL, **kw) -> dict:
+        """Run the variable-length transactions in batches (batch_off: n+1
+        transaction offsets), one launch per batch or one persistent queue."""
+        boff = np.ascontiguousarray(batch_off, dtype=np.uint32)
+        p = self.params(scheme, **kw)
+        r = Result()
+        rc = self.lib.gcc_run_batches(self._h, C.byref(p), _ptr(boff), len(boff) - 1, mode,
+                                      C.byref(r))
+        self.last_result = r.as_dict()
+        self.n_tx = self.n_var
+        self._last_nconf = 1 if mode == BATCHES_QUEUE else len(boff) - 1
+        _check(rc, f"gcc_run_batches({scheme}) err_site={r.err_site}")
+        return r.as_dict()
+
+    def batch_stats(self):
+        n = self._last_nconf
+        wd, bs = np.zeros(n, dtype=np.int32), np.zeros(n, dtype=np.int32)
+        ms = np.zeros(n, dtype=np.float64)
+        _check(self.lib.gcc_get_batch_stats(self._h, _ptr(wd), _ptr(bs), _ptr(ms), n),
+               "gcc_get_batch_stats")
+        return wd, bs, ms
 
     def dump_table(self) -> np.ndarray:
         a = np.empty((self.rows, self.row_bytes), dtype=np.uint8)

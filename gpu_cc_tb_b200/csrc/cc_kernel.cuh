@@ -46,7 +46,7 @@ enum AttemptStatus : int { kCommit = 0, kAbort = 1, kGiveUp = 2 };
 // Where a bounded wait gave up (Counters::err_where).
 enum WaitSite : unsigned {
     W_LATCH = 1, W_TPL_WD, W_TO_READ, W_MVCC_READ, W_SILO_READ, W_TICTOC_READ,
-    W_TICTOC_EXT, W_TURN, W_RETRY, W_CAS
+    W_TICTOC_EXT, W_TURN, W_RETRY, W_CAS, W_QUEUE
 };
 
 // ---------------------------------------------------------------------------
@@ -80,21 +80,24 @@ struct Group {
         }
         return v;
     }
-    GCC_D unsigned orv(unsigned v) const {
+    GCC_D unsigned long long orv(unsigned long long v) const {
 #pragma unroll
         for (int o = G / 2; o > 0; o >>= 1) v |= __shfl_xor_sync(mask, v, o, G);
         return v;
     }
 };
 
-// Per-transaction lane state: lane owns ops i = glane + k*G, k < K.
-template <int G>
+// Per-transaction lane state: lane owns ops i = glane + k*G, k < K, of a
+// transaction of at most MO requests.
+template <int G_, int MO>
 struct TxOps {
-    static constexpr int K = (kMaxOps + G - 1) / G;
-    uint32_t n;            // requests in the transaction
-    uint32_t valid;        // bit k: op k exists
-    uint32_t isread;       // bit k: op k reads
-    uint32_t readmask;     // group-wide: bit i set if op i reads
+    static constexpr int G = G_;
+    static constexpr int MAXOPS = MO;
+    static constexpr int K = (MO + G - 1) / G;
+    uint32_t n;                // requests in the transaction
+    uint32_t valid;            // bit k: op k exists
+    uint32_t isread;           // bit k: op k reads
+    unsigned long long readmask;  // group-wide: bit i set if op i reads
     uint32_t row[K];
 };
 
@@ -110,7 +113,7 @@ GCC_D void wait_pause() { __nanosleep(20); }
 constexpr int kMaxChunks = 7;  // 16-byte chunks cover up to 14 words (112 B)
 
 GCC_D size_t slot_of(const KParams &p, uint64_t unit, uint32_t i) {
-    return ((size_t)unit * kMaxOps + i) * p.wslot;
+    return ((size_t)unit * p.slot_ops + i) * p.wslot;
 }
 // Stream a row image from `src` (16-byte L2 loads), folding its words into
 // the digest term `dt` of op i and copying it to the rowcopy scratch slot and
@@ -139,13 +142,13 @@ GCC_D void copy_image(const KParams &p, uint64_t *dst, const uint64_t *src) {
             __stcg((ulonglong2 *)dst + c, __ldcg((const ulonglong2 *)src + c));
 }
 // Last read op before op i (program order), -1 if none.
-GCC_D int rowcopy_src(uint32_t readmask, uint32_t i) {
-    uint32_t m = readmask & ((1u << i) - 1u);
-    return m ? 31 - __clz(m) : -1;
+GCC_D int rowcopy_src(unsigned long long readmask, uint32_t i) {
+    unsigned long long m = readmask & ((1ull << i) - 1ull);
+    return m ? 63 - __clzll((long long)m) : -1;
 }
 // Apply write op i of tx to `row` (GCC_WRITE_FIELD or GCC_WRITE_ROWCOPY).
 GCC_D void apply_write(const KParams &p, uint32_t row, uint32_t tx, uint64_t pos,
-                       uint32_t i, uint32_t readmask) {
+                       uint32_t i, unsigned long long readmask) {
     uint64_t *r = row_ptr(p, row);
     if (p.write_mode == GCC_WRITE_FIELD) {
         uint32_t f = write_field(p.write_seed, tx, i);
@@ -300,10 +303,10 @@ GCC_D int tpl_lock(const KParams &p, uint32_t row, uint32_t tx, bool rd) {
 // reference does, so that competing transactions cannot keep aborting each
 // other. Both apply the scheme's rule: a conflict means abort (no-wait) or
 // wait-or-die by transaction age (wait-die).
-template <int G, bool WD, bool SLOW>
-GCC_D int attempt_tpl(const KParams &p, const Group<G> &g, const TxOps<G> &s, uint32_t tx,
+template <int G, bool WD, bool SLOW, class TX>
+GCC_D int attempt_tpl(const KParams &p, const Group<G> &g, const TX &s, uint32_t tx,
                       uint64_t pos, unsigned long long &dg, Clocks &ck, bool ordered) {
-    constexpr int K = TxOps<G>::K;
+    constexpr int K = TX::K;
     uint32_t held = 0, pending = s.valid;
     bool fail = false, err = false;
     uint32_t obst = kNoRow;  // row whose lock request failed
@@ -463,10 +466,10 @@ GCC_D int to_write(const KParams &p, uint32_t row, uint64_t ts, unsigned long lo
     return O_DONE;
 }
 
-template <int G, bool SLOW>
-GCC_D int attempt_to(const KParams &p, const Group<G> &g, const TxOps<G> &s, uint32_t tx,
+template <int G, bool SLOW, class TX>
+GCC_D int attempt_to(const KParams &p, const Group<G> &g, const TX &s, uint32_t tx,
                      uint64_t pos, unsigned long long &dg, Clocks &ck, bool ordered) {
-    constexpr int K = TxOps<G>::K;
+    constexpr int K = TX::K;
     unsigned long long ts = 0;
     if (g.glane == 0) {
         long long c0 = clock64();
@@ -622,10 +625,10 @@ GCC_D int mvcc_read(const KParams &p, uint32_t row, uint64_t ts, uint32_t tx, ui
     return r;
 }
 
-template <int G, bool SLOW>
-GCC_D int attempt_mvcc(const KParams &p, const Group<G> &g, const TxOps<G> &s, uint32_t tx,
+template <int G, bool SLOW, class TX>
+GCC_D int attempt_mvcc(const KParams &p, const Group<G> &g, const TX &s, uint32_t tx,
                        uint64_t pos, unsigned long long &dg, Clocks &ck, bool ordered) {
-    constexpr int K = TxOps<G>::K;
+    constexpr int K = TX::K;
     unsigned long long ts = 0;
     if (g.glane == 0) {
         long long c0 = clock64();
@@ -695,7 +698,7 @@ GCC_D int attempt_mvcc(const KParams &p, const Group<G> &g, const TxOps<G> &s, u
         uint32_t row = s.row[k];
         // push the current base row as the version it replaces, link it,
         // then install the new base row and publish (uncommitted -> 0)
-        uint32_t node = (uint32_t)(pos * kMaxOps + i);
+        uint32_t node = (uint32_t)(pos * p.slot_ops + i);
         copy_image(p, p.ver_data + (size_t)node * p.wslot, row_ptr(p, row));
         p.ver_ts[node] = prev[k];
         p.ver_prev[node] = ld_cg(p.turn + row);
@@ -761,11 +764,11 @@ GCC_D int occ_lock(const KParams &p, uint32_t row, unsigned long long lockbit,
 // Lock the write set, no-wait (silo.cuh:268-281, tictoc.cuh:269-282). First
 // attempts lock in parallel; retries lock one request at a time in request
 // order. `cts` accumulates f(word before locking) over the locked words.
-template <int G, bool SLOW, bool TICTOC>
-GCC_D void occ_lock_writes(const KParams &p, const Group<G> &g, const TxOps<G> &s,
+template <int G, bool SLOW, bool TICTOC, class TX>
+GCC_D void occ_lock_writes(const KParams &p, const Group<G> &g, const TX &s,
                            uint32_t writes, bool ordered, uint32_t &held,
                            unsigned long long &cts, bool &fail, bool &err, uint32_t &obst) {
-    constexpr int K = TxOps<G>::K;
+    constexpr int K = TX::K;
     const unsigned long long lockbit = TICTOC ? tictoc::kLock : silo::kLock;
     if (!ordered) {
 #pragma unroll
@@ -804,10 +807,10 @@ GCC_D void occ_lock_writes(const KParams &p, const Group<G> &g, const TxOps<G> &
     }
 }
 
-template <int G, bool SLOW>
-GCC_D int attempt_silo(const KParams &p, const Group<G> &g, const TxOps<G> &s, uint32_t tx,
+template <int G, bool SLOW, class TX>
+GCC_D int attempt_silo(const KParams &p, const Group<G> &g, const TX &s, uint32_t tx,
                        uint64_t pos, unsigned long long &dg, Clocks &ck, bool ordered) {
-    constexpr int K = TxOps<G>::K;
+    constexpr int K = TX::K;
     unsigned long long rec[K];
     uint32_t reads = s.valid & s.isread, writes = s.valid & ~s.isread;
     uint32_t pending = reads, held = 0;
@@ -941,10 +944,10 @@ GCC_D int tictoc_extend(const KParams &p, uint32_t row, unsigned long long rwts,
     return O_ERR;
 }
 
-template <int G, bool SLOW>
-GCC_D int attempt_tictoc(const KParams &p, const Group<G> &g, const TxOps<G> &s, uint32_t tx,
+template <int G, bool SLOW, class TX>
+GCC_D int attempt_tictoc(const KParams &p, const Group<G> &g, const TX &s, uint32_t tx,
                          uint64_t pos, unsigned long long &dg, Clocks &ck, bool ordered) {
-    constexpr int K = TxOps<G>::K;
+    constexpr int K = TX::K;
     unsigned long long rw[K], rr[K];
     uint32_t reads = s.valid & s.isread, writes = s.valid & ~s.isread;
     uint32_t pending = reads, held = 0;
@@ -1027,21 +1030,22 @@ GCC_D int attempt_tictoc(const KParams &p, const Group<G> &g, const TxOps<G> &s,
 // (gacco.cuh:156-175; GPUTx's rank launches become the same hand-off over the
 // (rank, tx) order, which also orders same-rank conflicts by tx index).
 // ===========================================================================
-template <int G>
-GCC_D int attempt_ordered(const KParams &p, const Group<G> &g, const TxOps<G> &s, uint32_t tx,
+template <int G, class TX>
+GCC_D int attempt_ordered(const KParams &p, const Group<G> &g, const TX &s, uint32_t tx,
                           uint64_t pos, unsigned long long &dg, Clocks &ck, bool ordered) {
-    constexpr int K = TxOps<G>::K;
+    constexpr int K = TX::K;
     uint32_t mypos[K];
 #pragma unroll
     for (int k = 0; k < K; ++k)
-        mypos[k] = ((s.valid >> k) & 1u) ? p.op_pos[pos * kMaxOps + g.glane + k * G] : 0u;
-    uint32_t pending = s.valid, done_ops = 0;
+        mypos[k] = ((s.valid >> k) & 1u) ? p.op_pos[pos * p.slot_ops + g.glane + k * G] : 0u;
+    uint32_t pending = s.valid;
+    unsigned long long done_ops = 0;
     const bool rowcopy = p.write_mode == GCC_WRITE_ROWCOPY;
     uint64_t t0 = gtimer();
     bool first = true;
     long long cw = 0;
     while (true) {
-        uint32_t mine = 0;
+        unsigned long long mine = 0;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             if (!((pending >> k) & 1u)) continue;
@@ -1049,7 +1053,7 @@ GCC_D int attempt_ordered(const KParams &p, const Group<G> &g, const TxOps<G> &s
             bool rd = (s.isread >> k) & 1u;
             if (!rd && rowcopy) {
                 int src = rowcopy_src(s.readmask, i);
-                if (src >= 0 && !((done_ops >> src) & 1u)) continue;
+                if (src >= 0 && !((done_ops >> src) & 1ull)) continue;
             }
             // acquire: the predecessor's access to the row is visible
             if (ld_acquire(p.turn + s.row[k]) != mypos[k]) continue;
@@ -1061,7 +1065,7 @@ GCC_D int attempt_ordered(const KParams &p, const Group<G> &g, const TxOps<G> &s
             // release: this access comes before the successor's
             st_release(p.turn + s.row[k], mypos[k] + 1u);
             pending &= ~(1u << k);
-            mine |= 1u << i;
+            mine |= 1ull << i;
         }
         done_ops |= g.orv(mine);
         if (rowcopy) g.sync();
@@ -1081,8 +1085,8 @@ GCC_D int attempt_ordered(const KParams &p, const Group<G> &g, const TxOps<G> &s
     return kCommit;
 }
 
-template <int SCH, int G>
-GCC_D int attempt(const KParams &p, const Group<G> &g, const TxOps<G> &s, uint32_t tx,
+template <int SCH, int G, class TX>
+GCC_D int attempt(const KParams &p, const Group<G> &g, const TX &s, uint32_t tx,
                   uint64_t pos, unsigned long long &dg, Clocks &ck, bool ordered) {
     if constexpr (SCH == S_TPL_NW) return attempt_tpl<G, false, false>(p, g, s, tx, pos, dg, ck, ordered);
     else if constexpr (SCH == S_TPL_WD) return attempt_tpl<G, true, false>(p, g, s, tx, pos, dg, ck, ordered);
@@ -1104,7 +1108,7 @@ __host__ __device__ constexpr bool is_ordered(int s) { return s == S_GACCO || s 
 // ===========================================================================
 // The persistent transaction kernel.
 // ===========================================================================
-template <int SCH, int G>
+template <int SCH, int G, int MO = kMaxOps>
 __global__ void __launch_bounds__(1024, 1) ycsb_kernel(const __grid_constant__ KParams p) {
     // Block-level histogram and metric sums (flushed once at exit) keep the
     // per-thread register budget for the transaction itself.
@@ -1115,7 +1119,8 @@ __global__ void __launch_bounds__(1024, 1) ycsb_kernel(const __grid_constant__ K
     __syncthreads();
 
     const Group<G> g;
-    constexpr int K = TxOps<G>::K;
+    using TX = TxOps<G, MO>;
+    constexpr int K = TX::K;
 
     // Positions come from 32 striped ticket counters (stripe j hands out
     // j, j + 32, j + 64, ... in increasing order, each counter on its own
@@ -1139,6 +1144,18 @@ __global__ void __launch_bounds__(1024, 1) ycsb_kernel(const __grid_constant__ K
                 if (++tried >= kTicketStripes) { stop = 1u; break; }
                 stripe = (stripe + 1) % kTicketStripes;
             }
+            // device queue: wait (bounded) until the position is admitted
+            if (!stop && p.queue_tail) {
+                const uint64_t tq = gtimer();
+                while (pos >= *p.queue_tail) {
+                    if (error_raised(p.ctr) || expired(tq, p.spin_limit_ns)) {
+                        set_error(p.ctr, GCC_ETIMEOUT, W_QUEUE);
+                        stop = 1u;
+                        break;
+                    }
+                    __nanosleep(256);
+                }
+            }
             if (error_raised(p.ctr)) stop = 1u;
         }
         stop = g.bcast(stop, 0);
@@ -1149,27 +1166,37 @@ __global__ void __launch_bounds__(1024, 1) ycsb_kernel(const __grid_constant__ K
         const uint64_t t_start = gtimer();
 
         // ---- requests and index probes --------------------------------
-        TxOps<G> s;
-        const gcc_ycsb_tx *T = p.txs + tx;
-        const unsigned long long n64 = __ldg(&T->request_cnt);
-        if (n64 > (unsigned long long)kMaxOps) {
+        TX s;
+        unsigned long long n64;
+        const gcc_ycsb_tx *T = nullptr;
+        uint32_t beg = 0;
+        if constexpr (MO == kMaxOps) {
+            T = p.txs + tx;
+            n64 = __ldg(&T->request_cnt);
+        } else {
+            beg = __ldg(p.tx_off + tx);
+            n64 = (unsigned long long)(__ldg(p.tx_off + tx + 1) - beg);
+        }
+        if (n64 > (unsigned long long)MO) {
             if (g.glane == 0) set_error(p.ctr, GCC_EFORMAT, 0);
             break;
         }
         s.n = (uint32_t)n64;
         s.valid = s.isread = 0;
         bool miss = false;
-        uint32_t myreads = 0;
+        unsigned long long myreads = 0;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             const uint32_t i = g.glane + k * G;
             s.row[k] = kNoRow;
             if (i < s.n) {
-                const int2 rq = __ldg((const int2 *)&T->requests[i]);
+                int2 rq;
+                if constexpr (MO == kMaxOps) rq = __ldg((const int2 *)&T->requests[i]);
+                else rq = __ldg((const int2 *)(p.reqs + beg + i));
                 s.valid |= 1u << k;
-                if (rq.x) { s.isread |= 1u << k; myreads |= 1u << i; }
+                if (rq.x) { s.isread |= 1u << k; myreads |= 1ull << i; }
                 if constexpr (is_ordered(SCH)) {
-                    s.row[k] = __ldg(p.op_row + pos * kMaxOps + i);
+                    s.row[k] = __ldg(p.op_row + pos * p.slot_ops + i);
                 } else {
                     s.row[k] = index_find(p, (uint32_t)rq.y);
                 }

@@ -36,6 +36,34 @@ int occupancy_one(int G, int block) {
     return e == cudaSuccess ? n : -1;
 }
 
+// Variable-length transactions (up to 64 requests): G in {4, 8, 16, 32}.
+template <int SCH>
+cudaError_t launch_var_one(int G, int grid, int block, const KParams &p, cudaStream_t st) {
+    switch (G) {
+        case 4: ycsb_kernel<SCH, 4, kMaxVarOps><<<grid, block, 0, st>>>(p); break;
+        case 8: ycsb_kernel<SCH, 8, kMaxVarOps><<<grid, block, 0, st>>>(p); break;
+        case 16: ycsb_kernel<SCH, 16, kMaxVarOps><<<grid, block, 0, st>>>(p); break;
+        case 32: ycsb_kernel<SCH, 32, kMaxVarOps><<<grid, block, 0, st>>>(p); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+template <int SCH>
+int occupancy_var_one(int G, int block) {
+    int n = 0;
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (G) {
+        case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ycsb_kernel<SCH, 4, kMaxVarOps>, block, 0); break;
+        case 8: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ycsb_kernel<SCH, 8, kMaxVarOps>, block, 0); break;
+        case 16: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ycsb_kernel<SCH, 16, kMaxVarOps>, block, 0); break;
+        case 32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ycsb_kernel<SCH, 32, kMaxVarOps>, block, 0); break;
+        default: break;
+    }
+    return e == cudaSuccess ? n : -1;
+}
+cudaError_t launch_var(int s, int G, int grid, int block, const KParams &p, cudaStream_t st);
+int occupancy_var(int s, int G, int block);
+
 // Declared per family; defined in cc_<family>.cu.
 cudaError_t launch_family_tpl(int s, int G, int grid, int block, const KParams &p, cudaStream_t st);
 cudaError_t launch_family_to(int s, int G, int grid, int block, const KParams &p, cudaStream_t st);

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include <cstdio>
 #include <cstring>
 #include <sstream>
@@ -104,7 +105,8 @@ struct gcc_engine {
     unsigned long long *sorted = nullptr;
     // transactions
     gcc_ycsb_tx *txs = nullptr;
-    uint64_t n_tx = 0, cap_tx = 0;
+    uint64_t n_rec = 0, cap_rec = 0;  // 16-request records loaded / capacity
+    uint64_t n_tx = 0, cap_tx = 0;    // transactions the per-tx outputs cover
     // per-row metadata
     unsigned long long *meta = nullptr;
     unsigned *latch = nullptr;
@@ -129,6 +131,24 @@ struct gcc_engine {
     std::vector<uint32_t *> scan_tmp;
     std::vector<uint64_t> scan_tmp_n;
     Counters *ctr = nullptr;
+    // variable-length transactions (CSR) and the batched executors
+    uint32_t *tx_off_d = nullptr;
+    gcc_ycsb_req *reqs_d = nullptr;
+    uint64_t n_var = 0, var_ops = 0, cap_var = 0, cap_var_ops = 0;
+    std::vector<uint32_t> tx_off_h;  // host copy of the offsets (batch classes)
+    unsigned long long *queue_tail = nullptr;
+    unsigned long long *stamps = nullptr;  // device time stamps of batched runs
+    uint64_t stamps_cap = 0;
+    struct Arm {
+        int wd, bs;
+        double ms_per_tx = 0;
+        uint64_t runs = 0;
+    };
+    std::map<int, std::vector<Arm>> tuner;  // batch class -> candidate configs
+    cudaGraphExec_t graph = nullptr;
+    std::vector<uint64_t> graph_key;
+    std::vector<int32_t> bstat_wd, bstat_bs;
+    std::vector<double> bstat_ms;
     // timing
     std::vector<cudaEvent_t> events;
     double last_kernel_ms = 0;
@@ -178,12 +198,13 @@ gcc_engine::~gcc_engine() {
     void *bufs[] = {table, hash_slots, sorted, txs, meta, latch, turn, digest, commit_hi,
                     commit_lo, tx_aborts, read_log, scratch, ver_ts, ver_prev, ver_data,
                     acc_key[0], acc_key[1], acc_val[0], acc_val[1], op_row, op_pos, order,
-                    tx_rank, sort_counts, ctr};
+                    tx_rank, sort_counts, ctr, tx_off_d, reqs_d, queue_tail, stamps};
     for (void *b : bufs)
         if (b) cudaFree(b);
     for (uint32_t *t : scan_tmp)
         if (t) cudaFree(t);
     for (cudaEvent_t ev : events) cudaEventDestroy(ev);
+    if (graph) cudaGraphExecDestroy(graph);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -192,6 +213,7 @@ KParams gcc_engine::base_params() const {
     memset(&p, 0, sizeof(p));
     p.txs = txs;
     p.n_tx = (uint32_t)n_tx;
+    p.slot_ops = kMaxOps;
     p.index_kind = desc.index_kind;
     p.hash_slots = hash_slots;
     p.hash_bucket_mask = hash_bucket_mask;
@@ -391,6 +413,7 @@ uint32_t gcc_row_bytes(int32_t layout) { return layout == GCC_LAYOUT_REF104 ? 10
 uint32_t gcc_row_stride(int32_t layout) { return layout == GCC_LAYOUT_REF104 ? 112u : 96u; }
 
 int gcc_create(const gcc_table_desc *d, gcc_engine **out) {
+    cudaGetLastError();  // a stale error of an earlier call is not ours
     if (!d || !out) return GCC_EINVAL;
     *out = nullptr;
     if (d->rows == 0 || d->rows >= 0xFFFFFFFFull) return GCC_EINVAL;
@@ -464,12 +487,16 @@ int gcc_create(const gcc_table_desc *d, gcc_engine **out) {
 void gcc_destroy(gcc_engine *e) { delete e; }
 
 int gcc_load_txs(gcc_engine *e, const gcc_ycsb_tx *txs, uint64_t n_tx) {
+    cudaGetLastError();  // a stale error of an earlier call is not ours
     if (!e || (!txs && n_tx)) return GCC_EINVAL;
     if (n_tx >= (1ull << 27)) return GCC_EINVAL;  // access ids must fit 31 bits
     cudaSetDevice(e->dev);
     int rc;
-    if (e->cap_tx < n_tx) {
+    if (e->cap_rec < n_tx) {
         if ((rc = e->alloc(&e->txs, n_tx * sizeof(gcc_ycsb_tx)))) return rc;
+        e->cap_rec = n_tx;
+    }
+    if (e->cap_tx < n_tx) {
         if ((rc = e->alloc(&e->digest, n_tx * 8))) return rc;
         if ((rc = e->alloc(&e->commit_hi, n_tx * 8))) return rc;
         if ((rc = e->alloc(&e->commit_lo, n_tx * 8))) return rc;
@@ -477,6 +504,7 @@ int gcc_load_txs(gcc_engine *e, const gcc_ycsb_tx *txs, uint64_t n_tx) {
         e->cap_tx = n_tx;
     }
     e->n_tx = n_tx;
+    e->n_rec = n_tx;
     e->have_run = false;
     if (n_tx) {
         cudaError_t ce = cudaMemcpyAsync(e->txs, txs, n_tx * sizeof(gcc_ycsb_tx),
@@ -487,6 +515,7 @@ int gcc_load_txs(gcc_engine *e, const gcc_ycsb_tx *txs, uint64_t n_tx) {
 }
 
 int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
+    cudaGetLastError();  // a stale error of an earlier call is not ours
     if (!e || !rp || !out) return GCC_EINVAL;
     memset(out, 0, sizeof(*out));
     const int s = gcc_scheme_id(rp->cc_scheme);
@@ -497,8 +526,9 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
     if (rp->block_size < 1 || rp->block_size > 32) return GCC_EINVAL;
     if (rp->batch_size < 1) return GCC_EINVAL;
     if (rp->write_mode != GCC_WRITE_FIELD && rp->write_mode != GCC_WRITE_ROWCOPY) return GCC_EINVAL;
-    if (!e->txs || e->n_tx == 0) return GCC_ESTATE;
+    if (!e->txs || e->n_rec == 0) return GCC_ESTATE;
     cudaSetDevice(e->dev);
+    e->n_tx = e->n_rec;  // outputs of this run cover the records
     const int G = 1 << rp->warp_density;
     const int block = rp->block_size * 32;
     const bool gputx = s == S_GPUTX;
@@ -670,10 +700,359 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
     return GCC_OK;
 }
 
+int gcc_load_var_txs(gcc_engine *e, const uint32_t *tx_off, const gcc_ycsb_req *reqs,
+                     uint64_t n_tx) {
+    cudaGetLastError();  // a stale error of an earlier call is not ours
+    if (!e || !tx_off || (!reqs && n_tx)) return GCC_EINVAL;
+    if (n_tx == 0 || n_tx >= (1ull << 27)) return GCC_EINVAL;
+    if (tx_off[0] != 0) return GCC_EINVAL;
+    for (uint64_t t = 0; t < n_tx; ++t)
+        if (tx_off[t + 1] < tx_off[t] || tx_off[t + 1] - tx_off[t] > (uint32_t)kMaxVarOps)
+            return GCC_EFORMAT;
+    const uint64_t ops = tx_off[n_tx];
+    cudaSetDevice(e->dev);
+    int rc;
+    if (e->cap_var < n_tx) {
+        if ((rc = e->alloc(&e->tx_off_d, (n_tx + 1) * 4))) return rc;
+        e->cap_var = n_tx;
+    }
+    if (e->cap_var_ops < ops) {
+        if ((rc = e->alloc(&e->reqs_d, ops * sizeof(gcc_ycsb_req)))) return rc;
+        e->cap_var_ops = ops;
+    }
+    if (e->cap_tx < n_tx) {
+        if ((rc = e->alloc(&e->digest, n_tx * 8))) return rc;
+        if ((rc = e->alloc(&e->commit_hi, n_tx * 8))) return rc;
+        if ((rc = e->alloc(&e->commit_lo, n_tx * 8))) return rc;
+        if ((rc = e->alloc(&e->tx_aborts, n_tx * 4))) return rc;
+        e->cap_tx = n_tx;
+    }
+    if (!e->queue_tail && (rc = e->alloc(&e->queue_tail, 8))) return rc;
+    cudaError_t ce = cudaMemcpyAsync(e->tx_off_d, tx_off, (n_tx + 1) * 4, cudaMemcpyHostToDevice, e->stream);
+    if (ce == cudaSuccess && ops)
+        ce = cudaMemcpyAsync(e->reqs_d, reqs, ops * sizeof(gcc_ycsb_req), cudaMemcpyHostToDevice, e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    if (ce != cudaSuccess) return e->fail_cuda(ce);
+    e->tx_off_h.assign(tx_off, tx_off + n_tx + 1);
+    e->n_var = n_tx;
+    e->var_ops = ops;
+    e->have_run = false;
+    if (e->graph) {
+        cudaGraphExecDestroy(e->graph);
+        e->graph = nullptr;
+        e->graph_key.clear();
+    }
+    return GCC_OK;
+}
+
+namespace {
+
+bool var_scheme(int s) {
+    return s == S_TPL_NW || s == S_TPL_WD || s == S_TO || s == S_SILO || s == S_TICTOC || s == S_MVCC;
+}
+
+// Autotuner candidates (warp_density, block_size).
+const int kArms[][2] = {{5, 32}, {5, 16}, {4, 32}, {4, 16}, {3, 32}, {3, 16}};
+
+// Batch class: log2 of the batch size and the mean requests per tx in
+// steps of 8.
+int batch_class(const std::vector<uint32_t> &off, uint64_t t0, uint64_t t1) {
+    uint64_t n = t1 - t0;
+    int lg = 0;
+    while ((1ull << (lg + 1)) <= n) ++lg;
+    uint64_t ops = off[t1] - off[t0];
+    int ob = (int)(n ? (ops / n) / 8 : 0);
+    return lg * 16 + ob;
+}
+
+// Next config of a class: untried arms in order, then the fastest measured.
+gcc_engine::Arm *pick_arm(std::vector<gcc_engine::Arm> &arms) {
+    for (auto &a : arms)
+        if (a.runs == 0) return &a;
+    gcc_engine::Arm *best = &arms[0];
+    for (auto &a : arms)
+        if (a.ms_per_tx < best->ms_per_tx) best = &a;
+    return best;
+}
+
+__global__ void k_set_u64(unsigned long long *p, unsigned long long v) { *p = v; }
+
+}  // namespace
+
+int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *batch_off,
+                    uint64_t nb, int32_t mode, gcc_result *out) {
+    cudaGetLastError();  // a stale error of an earlier call is not ours
+    if (!e || !rp || !batch_off || !out || nb == 0) return GCC_EINVAL;
+    memset(out, 0, sizeof(*out));
+    const int s = gcc_scheme_id(rp->cc_scheme);
+    if (s < 0 || !var_scheme(s)) return GCC_EINVAL;
+    if (mode != GCC_BATCHES_SEQUENTIAL && mode != GCC_BATCHES_QUEUE) return GCC_EINVAL;
+    if (mode == GCC_BATCHES_QUEUE && s == S_MVCC) return GCC_EINVAL;
+    if (rp->warp_density < 2 || rp->warp_density > 5) return GCC_EINVAL;
+    if (rp->block_size < 1 || rp->block_size > 32) return GCC_EINVAL;
+    if (rp->write_mode != GCC_WRITE_FIELD) return GCC_EINVAL;
+    if (rp->backoff_ns < -1 || rp->backoff_ns > 100000) return GCC_EINVAL;
+    if (!e->n_var || !e->reqs_d) return GCC_ESTATE;
+    if (batch_off[0] != 0 || batch_off[nb] != e->n_var) return GCC_EINVAL;
+    for (uint64_t b = 0; b < nb; ++b)
+        if (batch_off[b + 1] <= batch_off[b]) return GCC_EINVAL;
+    cudaSetDevice(e->dev);
+    const bool autotune = (rp->flags & GCC_F_AUTOTUNE) != 0;
+    const bool use_graph = (rp->flags & GCC_F_GRAPH) != 0;
+    int rc;
+
+    // per-batch (or whole-run) configuration
+    const uint64_t nconf = mode == GCC_BATCHES_QUEUE ? 1 : nb;
+    std::vector<int> wd(nconf, rp->warp_density), bs(nconf, rp->block_size), cls(nconf, -1);
+    if (autotune) {
+        for (uint64_t b = 0; b < nconf; ++b) {
+            cls[b] = mode == GCC_BATCHES_QUEUE ? -1 : batch_class(e->tx_off_h, batch_off[b], batch_off[b + 1]);
+            auto &arms = e->tuner[cls[b]];
+            if (arms.empty())
+                for (auto &a : kArms) arms.push_back({a[0], a[1], 0.0, 0});
+        }
+        // one untried arm per class per run, so the runs of a class measure
+        // the arms one by one and the class settles on its fastest
+        std::map<int, gcc_engine::Arm *> chosen;
+        for (uint64_t b = 0; b < nconf; ++b) {
+            auto it = chosen.find(cls[b]);
+            if (it == chosen.end()) it = chosen.emplace(cls[b], pick_arm(e->tuner[cls[b]])).first;
+            wd[b] = it->second->wd;
+            bs[b] = it->second->bs;
+        }
+    }
+    uint64_t max_batch = 0;
+    for (uint64_t b = 0; b < nb; ++b) max_batch = std::max<uint64_t>(max_batch, batch_off[b + 1] - batch_off[b]);
+    if (s == S_MVCC && e->ver_units * kMaxOps < max_batch * kMaxVarOps) {
+        uint64_t nodes = max_batch * kMaxVarOps;
+        if ((rc = e->alloc(&e->ver_ts, nodes * 8))) return rc;
+        if ((rc = e->alloc(&e->ver_prev, nodes * 4))) return rc;
+        if ((rc = e->alloc(&e->ver_data, nodes * e->wslot * 8))) return rc;
+        e->ver_units = (nodes + kMaxOps - 1) / kMaxOps;
+    }
+    std::vector<int> grid(nconf), block(nconf);
+    for (uint64_t b = 0; b < nconf; ++b) {
+        block[b] = bs[b] * 32;
+        const int G = 1 << wd[b];
+        int occ = occupancy_var(s, G, block[b]);
+        if (occ <= 0) return GCC_EINVAL;
+        uint64_t n = mode == GCC_BATCHES_QUEUE ? e->n_var : batch_off[b + 1] - batch_off[b];
+        uint64_t want = (n * (uint64_t)G + block[b] - 1) / block[b];
+        grid[b] = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)occ * e->sm_count));
+    }
+    const uint64_t nst = 3 * nb + 4;
+    if (e->stamps_cap < nst) {
+        if ((rc = e->alloc(&e->stamps, nst * 8))) return rc;
+        e->stamps_cap = nst;
+    }
+
+    KParams p = e->base_params();
+    p.txs = nullptr;
+    p.tx_off = e->tx_off_d;
+    p.reqs = e->reqs_d;
+    p.n_tx = (uint32_t)e->n_var;
+    p.slot_ops = kMaxVarOps;
+    p.write_mode = rp->write_mode;
+    p.write_seed = rp->write_seed;
+    p.flags = rp->flags;
+    p.spin_limit_ns = rp->spin_limit_ns ? rp->spin_limit_ns : 4000000000ull;
+    p.backoff_ns = rp->backoff_ns < 0 ? 0u : (rp->backoff_ns == 0 ? 512u : (uint32_t)rp->backoff_ns);
+    p.ver_ts = e->ver_ts;
+    p.ver_prev = e->ver_prev;
+    p.ver_data = e->ver_data;
+
+    // graph key: everything the captured work depends on
+    std::vector<uint64_t> key = {(uint64_t)s, (uint64_t)mode, rp->flags, rp->write_seed,
+                                 p.spin_limit_ns, p.backoff_ns, (uint64_t)e->n_var, nb};
+    for (uint64_t b = 0; b <= nb; ++b) key.push_back(batch_off[b]);
+    for (uint64_t b = 0; b < nconf; ++b) key.push_back(((uint64_t)wd[b] << 32) | (uint64_t)bs[b]);
+
+    cudaStream_t st = e->stream;
+    unsigned long long *stamp = e->stamps;
+    auto mark = [&](int i) -> cudaError_t {
+        k_stamp<<<1, 1, 0, st>>>(stamp, i);
+        return cudaGetLastError();
+    };
+    const bool needs_reset = s == S_TO || s == S_MVCC ||
+                             !(rp->flags & GCC_F_NO_RESET);
+    auto enqueue = [&]() -> cudaError_t {
+        cudaError_t ce = cudaMemsetAsync(e->ctr, 0, sizeof(Counters), st);
+        if (ce == cudaSuccess) ce = mark(0);
+        if (mode == GCC_BATCHES_QUEUE) {
+            // one reset, every batch admitted to the queue, one persistent
+            // launch that drains positions 0..n_var-1 in order
+            if (ce == cudaSuccess) ce = cudaMemsetAsync(e->meta, 0, e->rows * 8, st);
+            if (ce == cudaSuccess) {
+                k_batch_prep<<<1, 32, 0, st>>>(e->ctr, s == S_TO ? 1 : 0);
+                k_set_u64<<<1, 1, 0, st>>>(e->queue_tail, e->n_var);
+                ce = cudaGetLastError();
+            }
+            KParams q = p;
+            q.batch_st = 0;
+            q.batch_n = (uint32_t)e->n_var;
+            q.queue_tail = e->queue_tail;
+            if (ce == cudaSuccess) ce = mark(3);
+            if (ce == cudaSuccess) ce = launch_var(s, 1 << wd[0], grid[0], block[0], q, st);
+            if (ce == cudaSuccess) ce = mark(4);
+        } else {
+            for (uint64_t b = 0; b < nb && ce == cudaSuccess; ++b) {
+                KParams q = p;
+                q.batch_st = batch_off[b];
+                q.batch_n = batch_off[b + 1] - batch_off[b];
+                ce = mark(3 + 3 * (int)b);
+                if (ce == cudaSuccess && (needs_reset || b == 0))
+                    ce = cudaMemsetAsync(e->meta, 0, e->rows * 8, st);
+                if (ce == cudaSuccess && s == S_MVCC) ce = cudaMemsetAsync(e->turn, 0xFF, e->rows * 4, st);
+                if (ce == cudaSuccess) {
+                    k_batch_prep<<<1, 32, 0, st>>>(e->ctr, (s == S_TO || s == S_MVCC) ? 1 : 0);
+                    ce = cudaGetLastError();
+                }
+                if (ce == cudaSuccess) ce = mark(4 + 3 * (int)b);
+                if (ce == cudaSuccess) ce = launch_var(s, 1 << wd[b], grid[b], block[b], q, st);
+                if (ce == cudaSuccess) ce = mark(5 + 3 * (int)b);
+            }
+        }
+        if (ce == cudaSuccess) ce = mark(2);
+        return ce;
+    };
+    cudaError_t ce = cudaSuccess;
+    if (use_graph) {
+        if (!e->graph || e->graph_key != key) {
+            if (e->graph) {
+                cudaGraphExecDestroy(e->graph);
+                e->graph = nullptr;
+            }
+            cudaGraph_t gr = nullptr;
+            ce = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+            if (ce == cudaSuccess) {
+                cudaError_t ce2 = enqueue();
+                ce = cudaStreamEndCapture(st, &gr);
+                if (ce2 != cudaSuccess) ce = ce2;
+            }
+            if (ce == cudaSuccess) ce = cudaGraphInstantiate(&e->graph, gr, 0);
+            if (gr) cudaGraphDestroy(gr);
+            if (ce != cudaSuccess) {
+                e->graph = nullptr;
+                return e->fail_cuda(ce);
+            }
+            e->graph_key = key;
+        }
+        ce = cudaGraphLaunch(e->graph, st);
+    } else {
+        ce = enqueue();
+    }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess) return e->fail_cuda(ce);
+
+    Counters hc;
+    ce = cudaMemcpy(&hc, e->ctr, sizeof(Counters), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return e->fail_cuda(ce);
+    std::vector<unsigned long long> ts(nst, 0);
+    ce = cudaMemcpy(ts.data(), e->stamps, nst * 8, cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return e->fail_cuda(ce);
+    auto span_ms = [&](int a, int b) { return ts[b] > ts[a] ? (double)(ts[b] - ts[a]) * 1e-6 : 0.0; };
+    e->have_run = true;
+    e->n_tx = e->n_var;  // outputs are indexed by the variable-length txs now
+    double proc = 0, pre = 0;
+    e->bstat_wd.assign(nconf, 0);
+    e->bstat_bs.assign(nconf, 0);
+    e->bstat_ms.assign(nconf, 0.0);
+    for (uint64_t b = 0; b < nconf; ++b) {
+        double kms;
+        if (mode == GCC_BATCHES_QUEUE) {
+            kms = span_ms(3, 4);
+        } else {
+            pre += span_ms(3 + 3 * (int)b, 4 + 3 * (int)b);
+            kms = span_ms(4 + 3 * (int)b, 5 + 3 * (int)b);
+        }
+        proc += kms;
+        e->bstat_wd[b] = wd[b];
+        e->bstat_bs[b] = bs[b];
+        e->bstat_ms[b] = kms;
+    }
+    const double tot_ms = span_ms(0, 2);
+    if (autotune && !hc.err) {
+        // feed the tuner: kernel ms per transaction of each class's arm
+        std::map<int, std::pair<double, uint64_t>> agg;
+        for (uint64_t b = 0; b < nconf; ++b) {
+            uint64_t n = mode == GCC_BATCHES_QUEUE ? e->n_var : batch_off[b + 1] - batch_off[b];
+            auto &a = agg[cls[b]];
+            a.first += e->bstat_ms[b];
+            a.second += n;
+        }
+        for (auto &kv : agg) {
+            auto &arms = e->tuner[kv.first];
+            for (auto &a : arms) {
+                if (a.wd != wd[0] && mode == GCC_BATCHES_QUEUE) continue;
+                bool match = false;
+                for (uint64_t b = 0; b < nconf; ++b)
+                    if (cls[b] == kv.first && wd[b] == a.wd && bs[b] == a.bs) match = true;
+                if (!match) continue;
+                double v = kv.second.first / (double)kv.second.second;
+                a.ms_per_tx = a.runs ? 0.5 * (a.ms_per_tx + v) : v;
+                a.runs += 1;
+            }
+        }
+    }
+    e->last_kernel_ms = proc;
+    e->last_launches = nconf;
+    out->committed = hc.committed;
+    out->aborts = hc.aborts;
+    out->pre_s = pre / 1000.0;
+    out->proc_s = proc / 1000.0;
+    out->tot_s = tot_ms / 1000.0;
+    out->tx_per_s = tot_ms > 0 ? (double)hc.committed * 1000.0 / tot_ms : 0.0;
+    const double inv = 1.0 / ((double)e->n_var * (double)e->clock_khz);
+    out->ts_d = hc.ts_cycles * inv;
+    out->wait_d = hc.wait_cycles * inv;
+    out->abort_d = hc.abort_cycles * inv;
+    out->mng_d = hc.mng_cycles * inv;
+    out->tot_d = hc.tot_cycles * inv;
+    out->idx_d = hc.idx_cycles * inv;
+    out->batches = nb;
+    out->kernel_launches = mode == GCC_BATCHES_QUEUE ? 3 : 2 * nb;
+    out->max_attempts = hc.max_attempts;
+    out->err_site = hc.err_where;
+    uint64_t total = 0;
+    for (int i = 0; i < kHistBuckets; ++i) total += hc.hist[i];
+    auto edge = [](int b) -> double {
+        if (b < 16) return (double)b + 1.0;
+        int lg = b / 16 + 3, sub = b % 16;
+        return std::ldexp(16.0 + sub + 1.0, lg - 4);
+    };
+    auto pct = [&](double q) -> double {
+        if (!total) return 0.0;
+        uint64_t target = (uint64_t)std::ceil(q * (double)total), acc = 0;
+        for (int i = 0; i < kHistBuckets; ++i) {
+            acc += hc.hist[i];
+            if (acc >= target) return edge(i) / 1000.0;
+        }
+        return edge(kHistBuckets - 1) / 1000.0;
+    };
+    out->lat_p50_us = pct(0.50);
+    out->lat_p99_us = pct(0.99);
+    if (hc.err) return (int)hc.err;
+    if (hc.committed != e->n_var) return GCC_ESTATE;
+    return GCC_OK;
+}
+
+int gcc_get_batch_stats(gcc_engine *e, int32_t *wd, int32_t *bs, double *kms, uint64_t n) {
+    if (!e || !wd || !bs || !kms) return GCC_EINVAL;
+    if (!e->have_run || n > e->bstat_ms.size()) return GCC_ESTATE;
+    for (uint64_t i = 0; i < n; ++i) {
+        wd[i] = e->bstat_wd[i];
+        bs[i] = e->bstat_bs[i];
+        kms[i] = e->bstat_ms[i];
+    }
+    return GCC_OK;
+}
+
 int gcc_run_checked(gcc_engine *e, const gcc_run_params *rp, gcc_result *out, int *verdict) {
+    cudaGetLastError();  // a stale error of an earlier call is not ours
     if (!e || !rp || !out || !verdict) return GCC_EINVAL;
     *verdict = 0;
-    if (!e->txs || e->n_tx == 0) return GCC_ESTATE;
+    if (!e->txs || e->n_rec == 0) return GCC_ESTATE;
+    e->n_tx = e->n_rec;
     cudaSetDevice(e->dev);
     const size_t tbytes = e->rows * e->stride;
     const uint64_t n = e->n_tx;

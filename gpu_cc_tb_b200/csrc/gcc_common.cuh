@@ -13,6 +13,7 @@
 namespace gcc {
 
 constexpr int kMaxOps = 16;              // requests per gen_ycsb record
+constexpr int kMaxVarOps = 64;           // requests per variable-length transaction
 constexpr uint32_t kNoRow = 0xFFFFFFFFu; // index miss / padding op
 constexpr uint64_t kGolden = 0x9E3779B97F4A7C15ull;
 
@@ -123,10 +124,15 @@ GCC_HD uint32_t hist_bucket(uint64_t ns) {
 // Kernel parameter block.
 // ---------------------------------------------------------------------------
 struct KParams {
-    const gcc_ycsb_tx *txs;     // all loaded transactions
+    const gcc_ycsb_tx *txs;     // all loaded transactions (16-request records)
+    const uint32_t *tx_off;     // variable-length transactions: requests of tx t
+    const gcc_ycsb_req *reqs;   //   are reqs[tx_off[t] .. tx_off[t+1]) (else null)
     uint32_t n_tx;              // loaded transactions
+    uint32_t slot_ops;          // request slots per position / tx (16 or 64)
     uint32_t batch_st;          // first position of this launch
     uint32_t batch_n;           // positions in this launch
+    const volatile unsigned long long *queue_tail;  // admitted positions (device
+                                // queue; null: all batch_n are admitted)
     const uint32_t *order;      // position -> tx id (null: batch_st + pos)
     // index
     int32_t index_kind;

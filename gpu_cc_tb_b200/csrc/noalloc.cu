@@ -89,6 +89,7 @@ extern "C" int gcc_run_tpl_nw_noalloc(const gcc_ycsb_tx *txs, uint64_t n_tx, voi
     memset(&p, 0, sizeof(p));
     p.txs = txs;
     p.n_tx = (uint32_t)n_tx;
+    p.slot_ops = gcc::kMaxOps;
     p.batch_st = 0;
     p.batch_n = (uint32_t)n_tx;
     p.index_kind = GCC_INDEX_DIRECT;  // keys are row ids

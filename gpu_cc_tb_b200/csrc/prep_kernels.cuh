@@ -309,6 +309,14 @@ __global__ void k_count_diff(const unsigned long long *a, const unsigned long lo
     if (d) atomicAdd(diff, d);
 }
 
+// Device-side time stamp (%globaltimer, ns) into slots[i]: timing that also
+// works inside a captured CUDA graph.
+__global__ void k_stamp(unsigned long long *slots, int i) {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    slots[i] = t;
+}
+
 // Per-launch counter reset: ticket stripes = 0 and, for TO/MVCC, ts = 1
 // (NaiveTSAllocator_CPU::Init, include/timestamp.cuh:76-80).
 __global__ void k_batch_prep(Counters *c, int reset_ts) {

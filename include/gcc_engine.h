@@ -164,6 +164,18 @@ int gcc_gen_ycsb(uint64_t rows, uint64_t n_tx, double theta, double read_ratio,
                  uint64_t seed, int32_t dedup, int32_t key_base,
                  int32_t threads, gcc_ycsb_tx *out);
 
+/* Variable-length transactions (no counterpart in the reference's 136-byte
+ * format, which caps a transaction at 16 requests): transaction t owns
+ * requests reqs[tx_off[t] .. tx_off[t+1]), 1..64 of them, distinct keys in
+ * ascending order. The offsets are a pure function of (seed, tx) with
+ * min_ops..max_ops requests per transaction; the requests follow gen_ycsb's
+ * rules (Zipf keys, read probability, repeats redrawn, key order). */
+int gcc_gen_ycsb_var_offsets(uint64_t n_tx, uint32_t min_ops, uint32_t max_ops,
+                             uint64_t seed, uint32_t *tx_off /* n_tx + 1 */);
+int gcc_gen_ycsb_var(uint64_t rows, uint64_t n_tx, double theta, double read_ratio,
+                     uint64_t seed, int32_t key_base, int32_t threads,
+                     const uint32_t *tx_off, gcc_ycsb_req *reqs);
+
 /* Engine lifetime (Table_CPU::InitData + AddIndex + DB_CPU::ToGPU). */
 int gcc_create(const gcc_table_desc *desc, gcc_engine **out);
 void gcc_destroy(gcc_engine *e);
@@ -188,6 +200,40 @@ int gcc_run_checked(gcc_engine *e, const gcc_run_params *p, gcc_result *out,
 /* Reference output line (ExecInfo::Analyse CSV columns) for a result. */
 int gcc_format_line(const gcc_run_params *p, const gcc_result *r, char *buf,
                     size_t buf_bytes);
+
+/* ---- batched execution of variable-length transactions ------------------
+ * Upload n_tx variable-length transactions (tx_off: n_tx + 1 offsets into
+ * reqs; at most 64 requests each). They replace nothing loaded by
+ * gcc_load_txs; digests, aborts and commit keys of gcc_run_batches are read
+ * with the same getters (indexed by tx). */
+int gcc_load_var_txs(gcc_engine *e, const uint32_t *tx_off, const gcc_ycsb_req *reqs,
+                     uint64_t n_tx);
+
+/* Modes of gcc_run_batches. */
+#define GCC_BATCHES_SEQUENTIAL 0 /* one kernel launch per batch, batch after
+                                    batch, metadata reset per batch (the
+                                    reference's batch loop) */
+#define GCC_BATCHES_QUEUE 1      /* one persistent kernel drains every batch
+                                    from a device queue in admission order;
+                                    no per-batch barrier (tpl_nw, tpl_wd, to,
+                                    silo, tictoc) */
+/* Extra run flags of gcc_run_batches. */
+#define GCC_F_AUTOTUNE 16u /* choose warp_density / block_size per batch class
+                              (size, requests per tx) from measured runs */
+#define GCC_F_GRAPH 32u    /* capture the whole run in a CUDA graph once and
+                              replay it while the configuration is unchanged */
+
+/* Run the loaded variable-length transactions split into n_batches batches
+ * (batch b = transactions batch_off[b] .. batch_off[b+1]). Schemes: tpl_nw,
+ * tpl_wd, to, silo, tictoc, mvcc (sequential only); warp_density 2..5.
+ * Synchronous. */
+int gcc_run_batches(gcc_engine *e, const gcc_run_params *p, const uint32_t *batch_off,
+                    uint64_t n_batches, int32_t mode, gcc_result *out);
+
+/* Per-batch configuration and kernel time of the last gcc_run_batches
+ * (sequential mode; queue mode reports one entry for the whole run). */
+int gcc_get_batch_stats(gcc_engine *e, int32_t *warp_density, int32_t *block_size,
+                        double *kernel_ms, uint64_t n);
 
 /* Results of the last run / current state (device -> host copies). */
 int gcc_dump_table(gcc_engine *e, void *host_dst, uint64_t bytes); /* packed rows */

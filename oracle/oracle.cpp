@@ -91,6 +91,38 @@ int oracle_fill_table(uint64_t rows, int32_t layout, uint64_t seed, uint8_t *out
     return GCC_OK;
 }
 
+int oracle_replay_var(uint8_t *table, uint64_t rows, int32_t layout, const uint32_t *tx_off,
+                      const gcc_ycsb_req *reqs, uint64_t n_tx, const uint32_t *order,
+                      uint64_t n_order, int32_t write_mode, uint64_t write_seed,
+                      uint64_t *digests) {
+    Ctx c{table, rows, layout, rbytes(layout), rbytes(layout) / 8, write_mode, write_seed};
+    std::vector<uint8_t> item(c.rb);
+    for (uint64_t j = 0; j < n_order; ++j) {
+        uint32_t t = order ? order[j] : (uint32_t)j;
+        if (t >= n_tx) return GCC_EINVAL;
+        uint32_t n = tx_off[t + 1] - tx_off[t];
+        if (n > 64) return GCC_EFORMAT;
+        std::fill(item.begin(), item.end(), 0);
+        uint64_t dg = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            const gcc_ycsb_req &rq = reqs[tx_off[t] + i];
+            if (rq.key >= rows) return GCC_EKEY;
+            uint8_t *r = c.table + (uint64_t)rq.key * c.rb;
+            if (rq.read) {
+                for (uint32_t k = 0; k < c.words; ++k) dg += term(load_word(r + 8 * k), i, k);
+                memcpy(item.data(), r, c.rb);
+            } else if (c.write_mode == GCC_WRITE_FIELD) {
+                uint32_t f = (uint32_t)(h3(c.wseed, t, 2ull * i) % 10ull);
+                store_word(r + 8 * (1 + f), h3(c.wseed, t, 2ull * i + 1));
+            } else {
+                memcpy(r, item.data(), c.rb);
+            }
+        }
+        if (digests) digests[t] = dg;
+    }
+    return GCC_OK;
+}
+
 int oracle_replay(uint8_t *table, uint64_t rows, int32_t layout, const gcc_ycsb_tx *txs,
                   uint64_t n_tx, const uint32_t *order, uint64_t n_order, int32_t write_mode,
                   uint64_t write_seed, uint64_t *digests, uint8_t *read_log) {

@@ -44,6 +44,13 @@ int oracle_replay(uint8_t *table, uint64_t rows, int32_t layout, const gcc_ycsb_
                   uint64_t n_tx, const uint32_t *order, uint64_t n_order, int32_t write_mode,
                   uint64_t write_seed, uint64_t *digests, uint8_t *read_log);
 
+/* The same serial replay for variable-length transactions: tx t owns
+ * reqs[tx_off[t] .. tx_off[t+1]) (at most 64). */
+int oracle_replay_var(uint8_t *table, uint64_t rows, int32_t layout, const uint32_t *tx_off,
+                      const gcc_ycsb_req *reqs, uint64_t n_tx, const uint32_t *order,
+                      uint64_t n_order, int32_t write_mode, uint64_t write_seed,
+                      uint64_t *digests);
+
 /* GPUTx execution order: ranks per tx (reference rank function), and the
  * txs sorted by (rank, tx). */
 int oracle_gputx_order(const gcc_ycsb_tx *txs, uint64_t n_tx, uint64_t rows, uint32_t *ranks,

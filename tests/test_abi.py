@@ -121,3 +121,16 @@ def test_create_without_gpu_fails_cleanly(gcc):
     assert lib.gcc_create(C.byref(d), C.byref(h)) == -9  # GCC_ENODEV
     assert lib.gcc_load_txs(None, None, 0) == -1
     assert lib.gcc_run(None, None, None) == -1
+
+
+def test_variable_length_generator_rules(gcc):
+    off, reqs = g.gen_ycsb_var(5000, 3000, 0.8, 0.9, min_ops=4, max_ops=64, seed=3, threads=3)
+    cnt = np.diff(off.astype(np.int64))
+    assert cnt.min() >= 4 and cnt.max() <= 64
+    assert abs(cnt.mean() - 34) < 2
+    for t in range(0, 3000, 37):
+        k = reqs["key"][off[t]:off[t + 1]].astype(np.int64)
+        assert (np.diff(k) > 0).all() and k.max() < 5000
+    off2, reqs2 = g.gen_ycsb_var(5000, 3000, 0.8, 0.9, min_ops=4, max_ops=64, seed=3, threads=1)
+    assert np.array_equal(off, off2) and np.array_equal(reqs.view(np.uint8), reqs2.view(np.uint8))
+    assert abs(reqs["read"].mean() - 0.9) < 0.01
