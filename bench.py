@@ -10,6 +10,13 @@ kernels, gCCTB's tot_time definition, benchmark_cpu/ycsb.cu:249-291).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--scheme tpl_nw]
   python bench.py --impl reference ...   # the CPU executor on the host cores
+  python bench.py --workload batched ...  # 64 uneven batches, 4-64 requests/tx
+
+The batched workload: 64 consecutive batches with log-uniform sizes in
+[4096, 262144] transactions of 4-64 requests (uniform), theta 0.8, read ratio
+0.9, on the same table; the device-queue executor (one persistent kernel,
+CUDA graph, autotuned warp_density/block_size/transactions in flight) against
+the same batches launched one by one with plain kernels.
 
 Multi-GPU runs are independent replicas (the path does not shard): every
 rank runs the whole workload on its own GPU; value = all ranks' committed
@@ -41,7 +48,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--scheme", default="tpl_nw")
-    ap.add_argument("--theta", type=float, default=0.6)
+    ap.add_argument("--theta", type=float, default=None,
+                    help="Zipf theta (default 0.6 plain, 0.8 batched)")
     ap.add_argument("--read-ratio", type=float, default=0.9)
     ap.add_argument("--rows", type=int, default=10_485_760)
     ap.add_argument("--txs", type=int, default=1_048_576)
@@ -53,7 +61,14 @@ def parse():
     ap.add_argument("--cpu-threads", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweep", default="", help="comma list of extra schemes to time once")
-    return ap.parse_args()
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched"],
+                    help="plain: 1,048,576 x 16-request transactions in 65,536 batches; "
+                         "batched: 64 uneven batches of 4-64-request transactions")
+    ap.add_argument("--batches", type=int, default=64)
+    a = ap.parse_args()
+    if a.theta is None:
+        a.theta = 0.8 if a.workload == "batched" else 0.6
+    return a
 
 
 def peaks():
@@ -203,10 +218,140 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+def batched_workload(g, a):
+    """a.batches batches with log-uniform sizes in [4096, 262144]
+    transactions of 4-64 requests (uniform), Zipf theta, read ratio r, on
+    the a.rows-row table (seeded)."""
+    rng = np.random.default_rng(141919810)
+    sizes = np.exp(rng.uniform(np.log(4096), np.log(262144), a.batches)).astype(np.int64)
+    boff = np.zeros(a.batches + 1, dtype=np.uint32)
+    boff[1:] = np.cumsum(sizes)
+    off, reqs = g.gen_ycsb_var(a.rows, int(boff[-1]), a.theta, a.read_ratio, min_ops=4,
+                               max_ops=64, seed=141919810)
+    return boff, off, reqs
+
+
+def run_batched(a):
+    """Uneven batched workload: the device-queue executor (one persistent
+    kernel, CUDA graph, autotuned) against the same batches launched one by
+    one with plain kernels, and one by one with the per-batch tuner."""
+    from gpu_cc_tb_b200 import replicas
+    rank, ws, local, dist = replicas.init_from_env("nccl")
+    import torch
+    import gpu_cc_tb_b200 as g
+    boff, off, reqs = batched_workload(g, a)
+    n_tx, n_ops = len(off) - 1, int(off[-1])
+    reads = int(reqs["read"].sum())
+    alg = 8 * n_tx + 8 * n_ops + reads * (32 + 88) + (n_ops - reads) * (32 + 8)
+    pinned = torch.empty(reqs.nbytes, dtype=torch.uint8, pin_memory=True)
+    host_reqs = pinned.numpy().view(g.REQ_DTYPE)
+    host_reqs[:] = reqs
+    eng = g.Engine(a.rows, layout=g.LAYOUT_U64X11, index=g.INDEX_HASH, fill_seed=141919810,
+                   device=local, max_batch=int(np.diff(boff).max()))
+    eng.load_var_txs(off, host_reqs)
+    sch = a.scheme
+    tuned = dict(warp_density=a.wd, block_size=a.bs, flags=g.F_AUTOTUNE | g.F_GRAPH, write_seed=1)
+    plain = dict(warp_density=a.wd, block_size=a.bs, flags=0, write_seed=1)
+    warm_tuned = max(a.warmup, 9)  # the tuner measures its 8 arms, then settles
+    for _ in range(warm_tuned):
+        eng.run_batches(sch, boff, g.BATCHES_QUEUE, **tuned)
+    clocks = Clocks(local)
+    replicas.barrier(dist)
+    clocks.start()
+    dev_s, committed, aborts, kern_ms = 0.0, 0, 0, 0.0
+    lat50, lat99 = [], []
+    for _ in range(a.steps):
+        r = eng.run_batches(sch, boff, g.BATCHES_QUEUE, **tuned)
+        dev_s += r["tot_s"]
+        committed += r["committed"]
+        aborts += r["aborts"]
+        kern_ms += r["proc_s"] * 1000
+        lat50.append(r["lat_p50_us"])
+        lat99.append(r["lat_p99_us"])
+    replicas.barrier(dist)
+    clk = clocks.stop()
+    wd_q, bs_q, _ = eng.batch_stats()
+    act_q = eng.batch_active()
+    # the same batches one by one, plain kernels at the given knobs
+    for _ in range(min(a.warmup, 1)):
+        eng.run_batches(sch, boff, g.BATCHES_SEQUENTIAL, **plain)
+    base_s, base_c, base_launch = 0.0, 0, 0
+    for _ in range(a.steps):
+        r = eng.run_batches(sch, boff, g.BATCHES_SEQUENTIAL, **plain)
+        base_s += r["tot_s"]
+        base_c += r["committed"]
+        base_launch += r["kernel_launches"]
+    # one by one with the per-batch-class tuner and graph replay
+    for _ in range(warm_tuned):
+        eng.run_batches(sch, boff, g.BATCHES_SEQUENTIAL, **tuned)
+    seq_s, seq_c = 0.0, 0
+    for _ in range(a.steps):
+        r = eng.run_batches(sch, boff, g.BATCHES_SEQUENTIAL, **tuned)
+        seq_s += r["tot_s"]
+        seq_c += r["committed"]
+    # end to end through the public API: H2D of the requests from pinned
+    # memory, the queue run, D2H of every transaction's read digest
+    e2e_s = 0.0
+    dig = torch.empty(n_tx * 8, dtype=torch.uint8, pin_memory=True).numpy().view(np.uint64)
+    for _ in range(a.steps):
+        replicas.barrier(dist)
+        s0 = time.perf_counter()
+        eng.load_var_txs(off, host_reqs)
+        eng.run_batches(sch, boff, g.BATCHES_QUEUE, **tuned)
+        g.library().gcc_get_digests(eng._h, g.C.c_void_p(dig.ctypes.data), n_tx)
+        e2e_s += time.perf_counter() - s0
+    job = replicas.combine(dist, dev_s, committed, e2e_s, a.steps * n_tx)
+    if rank == 0:
+        hbm, kind = peaks()
+        launch_ms = kern_ms / a.steps
+        achieved = alg / (launch_ms / 1000) / 1e9
+        line = {
+            "metric": "committed tx/s", "value": job["value"], "unit": "tx/s", "n_gpus": ws,
+            "steps": a.steps, "warmup": warm_tuned,
+            "ms_per_step": 1000 * job["device_s_max"] / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded variable-length gen_ycsb)",
+            "config": {"workload": f"ycsb_batched_{a.batches}_uneven_batches_{n_tx}tx_4to64ops_"
+                                   f"theta{a.theta}_r{a.read_ratio}",
+                       "cc_scheme": sch, "rows": a.rows, "transactions": n_tx, "requests": n_ops,
+                       "batch_sizes": "log-uniform in [4096, 262144]", "ops_per_tx": "uniform 4-64",
+                       "theta": a.theta, "read_ratio": a.read_ratio,
+                       "executor": "one persistent kernel, device queue, CUDA graph, autotuned",
+                       "tuned_config": {"warp_density": int(wd_q[0]), "block_size": int(bs_q[0]),
+                                        "in_flight": int(act_q[0])},
+                       "l2": "inputs larger than L2 (1.0 GB table + requests)",
+                       "parallelism": f"replicas x{ws}"},
+            "one_by_one_plain": {"value": base_c / base_s, "unit": "tx/s",
+                                 "kernel_launches_per_step": base_launch // a.steps,
+                                 "config": {"warp_density": a.wd, "block_size": a.bs}},
+            "one_by_one_autotuned_graph": {"value": seq_c / seq_s, "unit": "tx/s"},
+            "speedup_vs_one_by_one_plain": (committed / dev_s) / (base_c / base_s),
+            "aborts_per_step": aborts / a.steps,
+            "abort_rate": aborts / max(1, aborts + committed),
+            "latency_us": {"p50": statistics.median(lat50), "p99": statistics.median(lat99)},
+            "e2e": {"value": job["e2e_value"], "unit": "tx/s",
+                    "h2d_bytes_per_step": int(reqs.nbytes + off.nbytes),
+                    "d2h_bytes_per_step": int(n_tx * 8)},
+            "gpu_launches": 3 * a.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None, "kernel": "ycsb_kernel (queue)",
+                         "peak_kind": kind, "alg_bytes_per_launch": alg, "launch_ms": launch_ms},
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+        return
+    if a.workload == "batched":
+        run_batched(a)
         return
     from gpu_cc_tb_b200 import replicas
     rank, ws, local, dist = replicas.init_from_env("nccl")

@@ -72,7 +72,8 @@ class RunParams(C.Structure):
     _fields_ = [("cc_scheme", C.c_char_p), ("warp_density", C.c_int32),
                 ("block_size", C.c_int32), ("batch_size", C.c_int32), ("flags", C.c_uint32),
                 ("write_mode", C.c_int32), ("backoff_ns", C.c_int32), ("write_seed", C.c_uint64),
-                ("spin_limit_ns", C.c_uint64)]
+                ("spin_limit_ns", C.c_uint64),
+                ("starve_limit", C.c_int32), ("max_active", C.c_int32)]
 
 
 class Result(C.Structure):
@@ -141,6 +142,7 @@ def library() -> C.CDLL:
         "gcc_run_batches": (C.c_int, [P, C.POINTER(RunParams), P, C.c_uint64, C.c_int32,
                                       C.POINTER(Result)]),
         "gcc_get_batch_stats": (C.c_int, [P, P, P, P, C.c_uint64]),
+        "gcc_get_batch_active": (C.c_int, [P, P, C.c_uint64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -234,10 +236,11 @@ class Engine:
 
     def params(self, scheme: str, warp_density: int = 5, block_size: int = 32,
                batch_size: int = 65536, flags: int = 0, write_mode: int = WRITE_FIELD,
-               write_seed: int = 1, spin_limit_ns: int = 0, backoff_ns: int = 0) -> RunParams:
+               write_seed: int = 1, spin_limit_ns: int = 0, backoff_ns: int = 0,
+               starve_limit: int = 0, max_active: int = 0) -> RunParams:
         self._scheme = scheme.encode()
         return RunParams(self._scheme, warp_density, block_size, batch_size, flags, write_mode,
-                         backoff_ns, write_seed, spin_limit_ns)
+                         backoff_ns, write_seed, spin_limit_ns, starve_limit, max_active)
 
     def run(self, scheme: str, **kw) -> dict:
         p = self.params(scheme, **kw)
@@ -290,6 +293,12 @@ class Engine:
         _check(self.lib.gcc_get_batch_stats(self._h, _ptr(wd), _ptr(bs), _ptr(ms), n),
                "gcc_get_batch_stats")
         return wd, bs, ms
+
+    def batch_active(self) -> np.ndarray:
+        """Transactions in flight of each entry of the last run_batches."""
+        a = np.zeros(self._last_nconf, dtype=np.uint64)
+        _check(self.lib.gcc_get_batch_active(self._h, _ptr(a), len(a)), "gcc_get_batch_active")
+        return a
 
     def dump_table(self) -> np.ndarray:
         a = np.empty((self.rows, self.row_bytes), dtype=np.uint8)

@@ -46,7 +46,7 @@ enum AttemptStatus : int { kCommit = 0, kAbort = 1, kGiveUp = 2 };
 // Where a bounded wait gave up (Counters::err_where).
 enum WaitSite : unsigned {
     W_LATCH = 1, W_TPL_WD, W_TO_READ, W_MVCC_READ, W_SILO_READ, W_TICTOC_READ,
-    W_TICTOC_EXT, W_TURN, W_RETRY, W_CAS, W_QUEUE
+    W_TICTOC_EXT, W_TURN, W_RETRY, W_CAS, W_QUEUE, W_STARVE
 };
 
 // ---------------------------------------------------------------------------
@@ -1137,6 +1137,17 @@ __global__ void __launch_bounds__(1024, 1) ycsb_kernel(const __grid_constant__ K
         unsigned long long pos = 0;
         unsigned stop = 0;
         if (g.glane == 0) {
+            // admission pause: while some transaction is starving (it has
+            // aborted starve_limit times), take no new transaction, so the
+            // contention around it drains and it commits. The pause is
+            // advisory: after spin_limit_ns admissions resume regardless.
+            if (p.starve_limit && ld_volatile(&p.ctr->starving) != 0u) {
+                const uint64_t tw = gtimer();
+                while (ld_volatile(&p.ctr->starving) != 0u) {
+                    if (error_raised(p.ctr) || expired(tw, p.spin_limit_ns)) break;
+                    __nanosleep(1000);
+                }
+            }
             while (true) {
                 unsigned long long t = atomicAdd(&p.ctr->tickets[stripe * 16], 1ull);
                 pos = t * kTicketStripes + stripe;
@@ -1216,12 +1227,43 @@ __global__ void __launch_bounds__(1024, 1) ycsb_kernel(const __grid_constant__ K
         Clocks ck{0, 0, 0};
         unsigned long long dg = 0, c_abort = 0;
         long long c_attempt = c_after_idx;
+        bool starving = false;
         while (true) {
             dg = 0;
             c_attempt = clock64();
             st = attempt<SCH, G>(p, g, s, tx, pos, dg, ck, attempts > 0);
             if (st != kAbort) break;
             ++attempts;
+            if (p.starve_limit && attempts == p.starve_limit) {
+                starving = true;
+                if (g.glane == 0) atomicAdd(&p.ctr->starving, 1u);
+            }
+            // A transaction still aborting after 4 x starve_limit attempts
+            // retries only while it holds the starvation token: the others
+            // at that stage wait between attempts, holding nothing, so the
+            // holder meets only the in-flight work below that stage, which
+            // drains (admissions are paused) or reaches it in turn. One
+            // holder at a time guarantees progress for transactions whose
+            // retries would otherwise keep invalidating each other.
+            if (starving && attempts >= 4u * p.starve_limit) {
+                unsigned bad = 0;
+                if (g.glane == 0) {
+                    const unsigned me = tx + 1u;
+                    const uint64_t tw = gtimer();
+                    while (true) {
+                        const unsigned h = atomicCAS(&p.ctr->starve_token, 0u, me);
+                        if (h == 0u || h == me) break;
+                        if (error_raised(p.ctr)) { bad = 1; break; }
+                        if (expired(tw, p.spin_limit_ns)) {
+                            set_error(p.ctr, GCC_ETIMEOUT, W_STARVE);
+                            bad = 1;
+                            break;
+                        }
+                        __nanosleep(1000);
+                    }
+                }
+                if (g.bcast(bad, 0)) { st = kGiveUp; break; }
+            }
             // After 8 failed attempts, a short random pause (up to
             // backoff_ns, at most a few microseconds) breaks the symmetric
             // retry patterns that lock-step warps can otherwise repeat
@@ -1237,6 +1279,10 @@ __global__ void __launch_bounds__(1024, 1) ycsb_kernel(const __grid_constant__ K
                 st = kGiveUp;
                 break;
             }
+        }
+        if (starving && g.glane == 0) {
+            atomicCAS(&p.ctr->starve_token, tx + 1u, 0u);
+            atomicSub(&p.ctr->starving, 1u);
         }
         if (st == kGiveUp) break;
         dg = g.sum(dg);

@@ -41,6 +41,16 @@ const SchemeName kSchemes[] = {
     {"slowto", S_SLOW_TO},      {"slowmvcc", S_SLOW_MVCC},
 };
 
+// Grid that holds at most max_active transactions of G lanes in CTAs of
+// `block` threads (0: no cap).
+uint64_t active_grid(int32_t max_active, int G, int block) {
+    if (max_active <= 0) return ~0ull;
+    return std::max<uint64_t>(1, ((uint64_t)max_active * G + block - 1) / block);
+}
+
+// starve_limit of gcc_run_params -> kernel value (0: off)
+uint32_t starve_param(int32_t v) { return v < 0 ? 0u : (v == 0 ? 32u : (uint32_t)v); }
+
 bool is_slow(int s) { return s >= S_SLOW_TPL_NW; }
 bool uses_ts(int s) { return s == S_TO || s == S_SLOW_TO || s == S_MVCC || s == S_SLOW_MVCC; }
 bool is_mvcc(int s) { return s == S_MVCC || s == S_SLOW_MVCC; }
@@ -140,7 +150,8 @@ struct gcc_engine {
     unsigned long long *stamps = nullptr;  // device time stamps of batched runs
     uint64_t stamps_cap = 0;
     struct Arm {
-        int wd, bs;
+        int wd, bs, div;     // grid = the full persistent grid / div
+        uint64_t active;     // transactions in flight under this arm
         double ms_per_tx = 0;
         uint64_t runs = 0;
     };
@@ -149,6 +160,7 @@ struct gcc_engine {
     std::vector<uint64_t> graph_key;
     std::vector<int32_t> bstat_wd, bstat_bs;
     std::vector<double> bstat_ms;
+    std::vector<uint64_t> bstat_active;
     // timing
     std::vector<cudaEvent_t> events;
     double last_kernel_ms = 0;
@@ -566,7 +578,9 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
 
     int occ = scheme_occupancy(s, G, block);
     if (occ <= 0) return GCC_EINVAL;  // block too large for this kernel
-    const uint64_t max_grid = (uint64_t)occ * e->sm_count;
+    if (rp->max_active < 0 || rp->starve_limit < -1) return GCC_EINVAL;
+    const uint64_t max_grid = std::min<uint64_t>((uint64_t)occ * e->sm_count,
+                                                 active_grid(rp->max_active, G, block));
 
     KParams p = e->base_params();
     p.write_mode = rp->write_mode;
@@ -576,6 +590,7 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
     p.wait_die = (s == S_TPL_WD || s == S_SLOW_TPL_WD) ? 1u : 0u;
     if (rp->backoff_ns < -1 || rp->backoff_ns > 100000) return GCC_EINVAL;
     p.backoff_ns = rp->backoff_ns < 0 ? 0u : (rp->backoff_ns == 0 ? 512u : (uint32_t)rp->backoff_ns);
+    p.starve_limit = starve_param(rp->starve_limit);
     p.scratch = rowcopy ? e->scratch : nullptr;
     p.read_log = want_log ? e->read_log : nullptr;
     p.ver_ts = e->ver_ts;
@@ -751,8 +766,11 @@ bool var_scheme(int s) {
     return s == S_TPL_NW || s == S_TPL_WD || s == S_TO || s == S_SILO || s == S_TICTOC || s == S_MVCC;
 }
 
-// Autotuner candidates (warp_density, block_size).
-const int kArms[][2] = {{5, 32}, {5, 16}, {4, 32}, {4, 16}, {3, 32}, {3, 16}};
+// Autotuner candidates (warp_density, block_size, grid divisor), tried in
+// this order: the densest groups first, then fewer transactions in flight,
+// then more.
+const int kArms[][3] = {{5, 32, 1}, {5, 32, 2}, {5, 32, 4}, {4, 32, 2},
+                        {5, 16, 1}, {4, 32, 1}, {3, 32, 2}, {3, 32, 1}};
 
 // Batch class: log2 of the batch size and the mean requests per tx in
 // steps of 8.
@@ -766,13 +784,22 @@ int batch_class(const std::vector<uint32_t> &off, uint64_t t0, uint64_t t1) {
 }
 
 // Next config of a class: untried arms in order, then the fastest measured.
+// An untried arm is skipped when a measured arm with no more transactions in
+// flight already ran over 2x slower than the best: under contention adding
+// transactions in flight only adds aborts, and one bad arm can cost 10-50x.
 gcc_engine::Arm *pick_arm(std::vector<gcc_engine::Arm> &arms) {
+    gcc_engine::Arm *best = nullptr;
     for (auto &a : arms)
-        if (a.runs == 0) return &a;
-    gcc_engine::Arm *best = &arms[0];
-    for (auto &a : arms)
-        if (a.ms_per_tx < best->ms_per_tx) best = &a;
-    return best;
+        if (a.runs && (!best || a.ms_per_tx < best->ms_per_tx)) best = &a;
+    for (auto &a : arms) {
+        if (a.runs) continue;
+        bool pruned = false;
+        for (auto &m : arms)
+            if (best && m.runs && m.active <= a.active && m.ms_per_tx > 2.0 * best->ms_per_tx)
+                pruned = true;
+        if (!pruned) return &a;
+    }
+    return best ? best : &arms[0];
 }
 
 __global__ void k_set_u64(unsigned long long *p, unsigned long long v) { *p = v; }
@@ -803,13 +830,21 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
 
     // per-batch (or whole-run) configuration
     const uint64_t nconf = mode == GCC_BATCHES_QUEUE ? 1 : nb;
+    if (rp->max_active < 0 || rp->starve_limit < -1) return GCC_EINVAL;
     std::vector<int> wd(nconf, rp->warp_density), bs(nconf, rp->block_size), cls(nconf, -1);
+    std::vector<int> dv(nconf, 1);
     if (autotune) {
         for (uint64_t b = 0; b < nconf; ++b) {
             cls[b] = mode == GCC_BATCHES_QUEUE ? -1 : batch_class(e->tx_off_h, batch_off[b], batch_off[b + 1]);
             auto &arms = e->tuner[cls[b]];
             if (arms.empty())
-                for (auto &a : kArms) arms.push_back({a[0], a[1], 0.0, 0});
+                for (auto &a : kArms) {
+                    const int G = 1 << a[0], block = a[1] * 32;
+                    const uint64_t full =
+                        (uint64_t)std::max(0, occupancy_var(s, G, block)) * e->sm_count;
+                    const uint64_t act = std::max<uint64_t>(1, full / a[2]) * (uint64_t)(block / G);
+                    arms.push_back({a[0], a[1], a[2], act, 0.0, 0});
+                }
         }
         // one untried arm per class per run, so the runs of a class measure
         // the arms one by one and the class settles on its fastest
@@ -819,6 +854,7 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
             if (it == chosen.end()) it = chosen.emplace(cls[b], pick_arm(e->tuner[cls[b]])).first;
             wd[b] = it->second->wd;
             bs[b] = it->second->bs;
+            dv[b] = it->second->div;
         }
     }
     uint64_t max_batch = 0;
@@ -838,7 +874,9 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
         if (occ <= 0) return GCC_EINVAL;
         uint64_t n = mode == GCC_BATCHES_QUEUE ? e->n_var : batch_off[b + 1] - batch_off[b];
         uint64_t want = (n * (uint64_t)G + block[b] - 1) / block[b];
-        grid[b] = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)occ * e->sm_count));
+        uint64_t cap = std::max<uint64_t>(1, (uint64_t)occ * e->sm_count / dv[b]);
+        if (!autotune) cap = std::min<uint64_t>(cap, active_grid(rp->max_active, G, block[b]));
+        grid[b] = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, cap));
     }
     const uint64_t nst = 3 * nb + 4;
     if (e->stamps_cap < nst) {
@@ -857,15 +895,17 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
     p.flags = rp->flags;
     p.spin_limit_ns = rp->spin_limit_ns ? rp->spin_limit_ns : 4000000000ull;
     p.backoff_ns = rp->backoff_ns < 0 ? 0u : (rp->backoff_ns == 0 ? 512u : (uint32_t)rp->backoff_ns);
+    p.starve_limit = starve_param(rp->starve_limit);
     p.ver_ts = e->ver_ts;
     p.ver_prev = e->ver_prev;
     p.ver_data = e->ver_data;
 
     // graph key: everything the captured work depends on
     std::vector<uint64_t> key = {(uint64_t)s, (uint64_t)mode, rp->flags, rp->write_seed,
-                                 p.spin_limit_ns, p.backoff_ns, (uint64_t)e->n_var, nb};
+                                 p.spin_limit_ns, p.backoff_ns, p.starve_limit, (uint64_t)e->n_var, nb};
     for (uint64_t b = 0; b <= nb; ++b) key.push_back(batch_off[b]);
-    for (uint64_t b = 0; b < nconf; ++b) key.push_back(((uint64_t)wd[b] << 32) | (uint64_t)bs[b]);
+    for (uint64_t b = 0; b < nconf; ++b)
+        key.push_back(((uint64_t)wd[b] << 48) | ((uint64_t)bs[b] << 32) | (uint64_t)grid[b]);
 
     cudaStream_t st = e->stream;
     unsigned long long *stamp = e->stamps;
@@ -957,6 +997,7 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
     e->bstat_wd.assign(nconf, 0);
     e->bstat_bs.assign(nconf, 0);
     e->bstat_ms.assign(nconf, 0.0);
+    e->bstat_active.assign(nconf, 0);
     for (uint64_t b = 0; b < nconf; ++b) {
         double kms;
         if (mode == GCC_BATCHES_QUEUE) {
@@ -969,6 +1010,7 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
         e->bstat_wd[b] = wd[b];
         e->bstat_bs[b] = bs[b];
         e->bstat_ms[b] = kms;
+        e->bstat_active[b] = (uint64_t)grid[b] * (uint64_t)(block[b] >> wd[b]);
     }
     const double tot_ms = span_ms(0, 2);
     if (autotune && !hc.err) {
@@ -986,7 +1028,8 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
                 if (a.wd != wd[0] && mode == GCC_BATCHES_QUEUE) continue;
                 bool match = false;
                 for (uint64_t b = 0; b < nconf; ++b)
-                    if (cls[b] == kv.first && wd[b] == a.wd && bs[b] == a.bs) match = true;
+                    if (cls[b] == kv.first && wd[b] == a.wd && bs[b] == a.bs && dv[b] == a.div)
+                        match = true;
                 if (!match) continue;
                 double v = kv.second.first / (double)kv.second.second;
                 a.ms_per_tx = a.runs ? 0.5 * (a.ms_per_tx + v) : v;
@@ -1033,6 +1076,13 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
     out->lat_p99_us = pct(0.99);
     if (hc.err) return (int)hc.err;
     if (hc.committed != e->n_var) return GCC_ESTATE;
+    return GCC_OK;
+}
+
+int gcc_get_batch_active(gcc_engine *e, uint64_t *active, uint64_t n) {
+    if (!e || !active) return GCC_EINVAL;
+    if (!e->have_run || n > e->bstat_active.size()) return GCC_ESTATE;
+    for (uint64_t i = 0; i < n; ++i) active[i] = e->bstat_active[i];
     return GCC_OK;
 }
 

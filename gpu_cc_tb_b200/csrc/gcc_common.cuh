@@ -105,6 +105,8 @@ struct Counters {
     unsigned int err;              // first error status (negative gcc code)
     unsigned int err_where;        // diagnostic: which wait gave up
     unsigned int max_attempts;     // most attempts of one transaction
+    unsigned int starving;         // transactions past the starvation limit
+    unsigned int starve_token;     // 0, or 1 + tx of the starving tx that retries
     unsigned int hist[kHistBuckets];
 };
 
@@ -171,6 +173,7 @@ struct KParams {
     uint32_t flags;
     uint32_t wait_die;
     uint32_t backoff_ns;        // 0: retry at once
+    uint32_t starve_limit;      // 0: no starvation control
 };
 
 // ---------------------------------------------------------------------------

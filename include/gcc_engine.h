@@ -121,6 +121,16 @@ typedef struct gcc_run_params {
                               each other indefinitely) */
     uint64_t write_seed;   /* seed of GCC_WRITE_FIELD values */
     uint64_t spin_limit_ns;/* bound of any single device wait; 0 = 4 s */
+    int32_t starve_limit;  /* attempts after which a transaction counts as
+                              starving: while one is, no new transaction is
+                              started (for at most spin_limit_ns), and past 4x
+                              this many attempts starving transactions retry
+                              one at a time (0: 32; -1: never) */
+    int32_t max_active;    /* cap on transactions in flight at once: the
+                              persistent grid holds at most this many (rounded
+                              up to whole CTAs); 0 = as many as the GPU holds.
+                              Under heavy contention fewer in flight abort
+                              less. With GCC_F_AUTOTUNE the tuner picks it. */
 } gcc_run_params;
 
 /* Fields 1-15 are the 15 columns of the reference's output line
@@ -234,6 +244,11 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *p, const uint32_t *batc
  * (sequential mode; queue mode reports one entry for the whole run). */
 int gcc_get_batch_stats(gcc_engine *e, int32_t *warp_density, int32_t *block_size,
                         double *kernel_ms, uint64_t n);
+
+/* Transactions in flight (persistent grid x transactions per CTA) of each
+ * entry of the last gcc_run_batches, entry for entry as gcc_get_batch_stats.
+ * No counterpart in the reference (its grid covers the whole batch). */
+int gcc_get_batch_active(gcc_engine *e, uint64_t *active, uint64_t n);
 
 /* Results of the last run / current state (device -> host copies). */
 int gcc_dump_table(gcc_engine *e, void *host_dst, uint64_t bytes); /* packed rows */

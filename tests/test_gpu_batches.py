@@ -64,8 +64,9 @@ def test_graph_replay_and_autotune(oracle, var_setup):
         assert res["committed"] == len(off) - 1
         check(oracle, eng, init, off, reqs, 5)
         wd, bs, ms = eng.batch_stats()
-        assert len(wd) == 4 and (ms > 0).all()
-        seen.update(zip(wd.tolist(), bs.tolist()))
+        act = eng.batch_active()
+        assert len(wd) == 4 and (ms > 0).all() and (act > 0).all()
+        seen.update(zip(wd.tolist(), bs.tolist(), act.tolist()))
     assert len(seen) >= 3  # the tuner explored several configurations
     for run in range(2):
         eng.upload_table(init)

@@ -29,11 +29,11 @@ def expected_order(oracle, scheme, eng, txs, rows):
 
 
 def run_and_check(oracle, eng, init, txs, scheme, wd, bs, batch, write_mode, layout,
-                  write_seed=99, read_log=False):
+                  write_seed=99, read_log=False, **kw):
     eng.upload_table(init)
     flags = g.F_COMMIT_LOG | (g.F_READ_LOG if read_log else 0)
     res = eng.run(scheme, warp_density=wd, block_size=bs, batch_size=batch, flags=flags,
-                  write_mode=write_mode, write_seed=write_seed, spin_limit_ns=SPIN_NS)
+                  write_mode=write_mode, write_seed=write_seed, spin_limit_ns=SPIN_NS, **kw)
     assert res["committed"] == len(txs)
     table = eng.dump_table()
     dg = eng.digests()
@@ -108,6 +108,22 @@ def test_scheme_parity_hot_rows(oracle, scheme):
     if scheme == "gputx":
         _, _, mx = oracle.gputx_order(txs, rows)
         assert res["rank_count"] == mx + 1
+
+
+@pytest.mark.parametrize("scheme", ["tpl_nw", "tpl_wd", "to", "mvcc", "silo", "tictoc"])
+def test_starvation_control_and_in_flight_cap(oracle, scheme):
+    # hot rows with an aggressive starvation limit (admission pause after 2
+    # aborts, one-at-a-time retries after 8) and with few transactions in
+    # flight: neither may change what commits or the serial equivalence
+    rows, layout = 64, g.LAYOUT_U64X11
+    txs = g.gen_ycsb(rows, 2048, 0.99, 0.5, seed=31, dedup=g.DEDUP_RESAMPLE, key_base=0)
+    init = oracle.fill_table(rows, layout, 9)
+    with g.Engine(rows, layout=layout, index=g.INDEX_DIRECT, fill_seed=9, max_batch=1024) as eng:
+        eng.load_txs(txs)
+        run_and_check(oracle, eng, init, txs, scheme, 5, 32, 1024, g.WRITE_FIELD, layout,
+                      starve_limit=2)
+        run_and_check(oracle, eng, init, txs, scheme, 3, 8, 1024, g.WRITE_FIELD, layout,
+                      starve_limit=-1, max_active=40)
 
 
 @pytest.mark.parametrize("scheme", ["tpl_nw", "tictoc", "gacco", "mvcc"])
