@@ -11,12 +11,19 @@ kernels, gCCTB's tot_time definition, benchmark_cpu/ycsb.cu:249-291).
   python bench.py [--gpus N] [--steps K] [--warmup W] [--scheme tpl_nw]
   python bench.py --impl reference ...   # the CPU executor on the host cores
   python bench.py --workload batched ...  # 64 uneven batches, 4-64 requests/tx
+  python bench.py --workload learned ...  # drifting contention, learned scheduling
 
 The batched workload: 64 consecutive batches with log-uniform sizes in
 [4096, 262144] transactions of 4-64 requests (uniform), theta 0.8, read ratio
 0.9, on the same table; the device-queue executor (one persistent kernel,
 CUDA graph, autotuned warp_density/block_size/transactions in flight) against
 the same batches launched one by one with plain kernels.
+
+The learned-scheduling workload: 256 batches of 65,536 transactions of 16
+requests on the same table, Zipf theta drifting linearly from 0.5 to 0.99
+and read ratio from 0.9 to 0.5 across the batches; the learned scheduler
+(BF16 MLP contention predictor, deferral into capped sub-batches, measured
+policy) against plain ordering on identical batches through the same driver.
 
 Multi-GPU runs are independent replicas (the path does not shard): every
 rank runs the whole workload on its own GPU; value = all ranks' committed
@@ -61,13 +68,17 @@ def parse():
     ap.add_argument("--cpu-threads", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweep", default="", help="comma list of extra schemes to time once")
-    ap.add_argument("--workload", default="plain", choices=["plain", "batched"],
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "learned"],
                     help="plain: 1,048,576 x 16-request transactions in 65,536 batches; "
-                         "batched: 64 uneven batches of 4-64-request transactions")
-    ap.add_argument("--batches", type=int, default=64)
+                         "batched: 64 uneven batches of 4-64-request transactions; "
+                         "learned: 256 drifting-contention batches, learned scheduling")
+    ap.add_argument("--batches", type=int, default=None,
+                    help="batches of the batched (64) / learned (256) workloads")
     a = ap.parse_args()
     if a.theta is None:
         a.theta = 0.8 if a.workload == "batched" else 0.6
+    if a.batches is None:
+        a.batches = 256 if a.workload == "learned" else 64
     return a
 
 
@@ -345,6 +356,128 @@ def run_batched(a):
         dist.destroy_process_group()
 
 
+def learned_workload(g, a):
+    """a.batches batches of 65,536 x 16-request transactions; theta drifts
+    linearly 0.5 -> 0.99 and the read ratio 0.9 -> 0.5 across batches."""
+    parts = []
+    nb = a.batches
+    for b in range(nb):
+        f = b / max(1, nb - 1)
+        parts.append(g.gen_ycsb(a.rows, a.batch, 0.5 + 0.49 * f, 0.9 - 0.4 * f, seed=141919810 + b,
+                                dedup=g.DEDUP_RESAMPLE, key_base=0))
+    return np.concatenate(parts)
+
+
+def run_learned(a):
+    """Learned contention scheduling against plain ordering on identical
+    batches, both through gcc_sched_run (the plain arm runs no predictor)."""
+    from gpu_cc_tb_b200 import replicas
+    rank, ws, local, dist = replicas.init_from_env("nccl")
+    import torch
+    import gpu_cc_tb_b200 as g
+    sch = a.scheme if a.scheme in g.SCHED_SCHEMES else "tpl_nw"
+    txs = learned_workload(g, a)
+    n = len(txs)
+    pinned = torch.empty(txs.nbytes, dtype=torch.uint8, pin_memory=True)
+    host_txs = pinned.numpy().view(g.TX_DTYPE)
+    host_txs[:] = txs
+    eng = g.Engine(a.rows, layout=g.LAYOUT_U64X11, index=g.INDEX_HASH, fill_seed=141919810,
+                   device=local, max_batch=a.batch)
+    eng.load_txs(host_txs)
+    kw = dict(warp_density=a.wd, block_size=a.bs, batch_size=a.batch, write_seed=1)
+    learned = g.Scheduler(eng, mode=g.SCHED_LEARNED, seed=7)
+    plain = g.Scheduler(eng, mode=g.SCHED_PLAIN)
+    for _ in range(a.warmup):
+        learned.run(sch, **kw)          # trains the network, settles the policy
+    plain.run(sch, **kw)
+    clocks = Clocks(local)
+    replicas.barrier(dist)
+    clocks.start()
+    dev_s, committed, aborts, launches, lat99 = 0.0, 0, 0, 0, []
+    res = []
+    for _ in range(a.steps):
+        r = learned.run(sch, **kw)
+        dev_s += r["tot_s"]
+        committed += r["committed"]
+        aborts += r["aborts"]
+        launches += r["kernel_launches"]
+        lat99.append(r["lat_p99_us"])
+        res.append(r)
+    replicas.barrier(dist)
+    clk = clocks.stop()
+    recs = learned.batches()
+    p_s, p_c, p_a, p_lat = 0.0, 0, 0, []
+    for _ in range(a.steps):
+        r = plain.run(sch, **kw)
+        p_s += r["tot_s"]
+        p_c += r["committed"]
+        p_a += r["aborts"]
+        p_lat.append(r["lat_p99_us"])
+    # the high-contention end: the last quarter of the batches (theta >= 0.87)
+    q0 = 3 * len(recs) // 4
+    hi_l = sum(b["committed"] for b in recs[q0:]) / (sum(b["ms"] for b in recs[q0:]) / 1e3)
+    precs = plain.batches()
+    hi_p = sum(b["committed"] for b in precs[q0:]) / (sum(b["ms"] for b in precs[q0:]) / 1e3)
+    e2e_s = 0.0
+    dig = torch.empty(n * 8, dtype=torch.uint8, pin_memory=True).numpy().view(np.uint64)
+    for _ in range(a.steps):
+        replicas.barrier(dist)
+        s0 = time.perf_counter()
+        eng.load_txs(host_txs)
+        learned.run(sch, **kw)
+        g.library().gcc_get_digests(eng._h, g.C.c_void_p(dig.ctypes.data), n)
+        e2e_s += time.perf_counter() - s0
+    job = replicas.combine(dist, dev_s, committed, e2e_s, a.steps * n)
+    if rank == 0:
+        last = res[-1]
+        hbm, kind = peaks()
+        alg, _, _ = algorithmic_bytes(txs)
+        kern_s = sum(r["proc_s"] for r in res) / a.steps
+        achieved = alg / kern_s / 1e9
+        line = {
+            "metric": "committed tx/s (learned vs plain CC, same GPU, 0 violations)",
+            "value": job["value"], "unit": "tx/s", "n_gpus": ws, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": 1000 * job["device_s_max"] / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded gen_ycsb per batch)",
+            "config": {"workload": f"ycsb_learned_{a.batches}x{a.batch}tx_16ops_theta0.5to0.99_"
+                                   f"r0.9to0.5", "cc_scheme": sch, "rows": a.rows,
+                       "transactions": n, "batch_size": a.batch, "warp_density": a.wd,
+                       "block_size": a.bs,
+                       "predictor": "MLP 66-128-128-1, BF16 weights, FP32 accumulation, "
+                                    "trained online on probe abort labels",
+                       "l2": "inputs larger than L2 (1.0 GB table + 2.3 GB transactions)",
+                       "parallelism": f"replicas x{ws}"},
+            "plain_ordering": {"value": p_c / p_s, "unit": "tx/s",
+                               "abort_rate": p_a / max(1, p_a + p_c),
+                               "p99_us": statistics.median(p_lat)},
+            "speedup_vs_plain": (committed / dev_s) / (p_c / p_s),
+            "high_contention_quarter": {"theta": ">= 0.87", "learned_tx_per_s": hi_l,
+                                        "plain_tx_per_s": hi_p, "speedup": hi_l / hi_p},
+            "abort_rate": aborts / max(1, aborts + committed),
+            "probe_abort_rate": last["probe_abort_rate"],
+            "sched_abort_rate": last["sched_abort_rate"],
+            "predictor": {"predict_ms": last["predict_ms"], "train_ms": last["train_ms"],
+                          "last_probe_loss": last["last_loss"]},
+            "latency_us": {"p99": statistics.median(lat99)},
+            "e2e": {"value": job["e2e_value"], "unit": "tx/s", "h2d_bytes_per_step": int(txs.nbytes),
+                    "d2h_bytes_per_step": int(n * 8)},
+            "gpu_launches": int(launches // a.steps),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None,
+                         "kernel": "ycsb_kernel (all launches of a pass)", "peak_kind": kind,
+                         "alg_bytes_per_pass": alg, "kernel_s_per_pass": kern_s},
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    learned.close()
+    plain.close()
+    eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -352,6 +485,9 @@ def main():
         return
     if a.workload == "batched":
         run_batched(a)
+        return
+    if a.workload == "learned":
+        run_learned(a)
         return
     from gpu_cc_tb_b200 import replicas
     rank, ws, local, dist = replicas.init_from_env("nccl")

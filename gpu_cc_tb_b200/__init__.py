@@ -97,6 +97,32 @@ class CommitRec(C.Structure):
 _LIB = None
 
 
+class SchedParams(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("explore_every", C.c_int32), ("probe_rows", C.c_int32),
+                ("train_steps", C.c_int32), ("minibatch", C.c_int32), ("lr", C.c_float),
+                ("defer_threshold", C.c_float), ("fixed_arm", C.c_int32), ("seed", C.c_uint64)]
+
+
+class SchedBatch(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("bucket", C.c_uint32), ("arm", C.c_uint32),
+                ("in_flight_cap", C.c_uint32), ("wait_die", C.c_uint32), ("probe", C.c_uint32),
+                ("deferred", C.c_uint64), ("pred_mean", C.c_float), ("label_mean", C.c_float),
+                ("loss", C.c_float), ("explored", C.c_uint32), ("ms", C.c_double),
+                ("committed", C.c_uint64), ("aborts", C.c_uint64)]
+
+
+class SchedResult(C.Structure):
+    _fields_ = [("run", Result), ("probed", C.c_uint64), ("deferred", C.c_uint64),
+                ("probe_tx_per_s", C.c_double), ("sched_tx_per_s", C.c_double),
+                ("probe_abort_rate", C.c_double), ("sched_abort_rate", C.c_double),
+                ("predict_ms", C.c_double), ("train_ms", C.c_double), ("last_loss", C.c_double)]
+
+
+SCHED_PLAIN, SCHED_LEARNED = 0, 1
+SCHED_FEAT_STRIDE = 72
+SCHED_SCHEMES = ["tpl_nw", "tpl_wd", "silo", "tictoc"]
+
+
 def library_path() -> Path:
     return Path(os.environ.get("GCC_LIB", LIB_PATH))
 
@@ -143,6 +169,18 @@ def library() -> C.CDLL:
                                       C.POINTER(Result)]),
         "gcc_get_batch_stats": (C.c_int, [P, P, P, P, C.c_uint64]),
         "gcc_get_batch_active": (C.c_int, [P, P, C.c_uint64]),
+        "gcc_sched_param_count": (C.c_uint64, []),
+        "gcc_sched_create": (C.c_int, [P, C.POINTER(SchedParams), C.POINTER(P)]),
+        "gcc_sched_destroy": (None, [P]),
+        "gcc_sched_run": (C.c_int, [P, C.POINTER(RunParams), C.POINTER(SchedResult)]),
+        "gcc_sched_batches": (C.c_int, [P, P, C.c_uint64]),
+        "gcc_sched_features": (C.c_int, [P, C.c_uint64, C.c_uint64, P]),
+        "gcc_sched_observe": (C.c_int, [P, C.c_uint64, C.c_uint64, C.c_int32]),
+        "gcc_sched_set_weights": (C.c_int, [P, P, C.c_uint64]),
+        "gcc_sched_get_weights": (C.c_int, [P, P, C.c_uint64]),
+        "gcc_sched_predict": (C.c_int, [P, P, C.c_uint64, P]),
+        "gcc_sched_gradient": (C.c_int, [P, P, P, C.c_uint64, P, C.POINTER(C.c_double)]),
+        "gcc_sched_train": (C.c_int, [P, P, P, C.c_uint64, C.c_int32, C.POINTER(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -340,3 +378,93 @@ class Engine:
         ms, n = C.c_double(), C.c_uint64()
         _check(self.lib.gcc_last_kernel_ms(self._h, C.byref(ms), C.byref(n)), "gcc_last_kernel_ms")
         return ms.value, n.value
+
+
+class Scheduler:
+    """Learned contention scheduling over an Engine's loaded 16-request
+    records (gcc_sched_*): a BF16 MLP predicts which transactions abort under
+    plain ordering; scheduled batches defer those into a capped sub-batch.
+    mode=SCHED_PLAIN runs every batch with plain ordering through the same
+    driver (the comparison arm)."""
+
+    def __init__(self, engine: "Engine", mode: int = SCHED_LEARNED, explore_every: int = 0,
+                 probe_rows: int = 0, train_steps: int = 0, minibatch: int = 0, lr: float = 0.0,
+                 defer_threshold: float = 0.0, fixed_arm: int = 0, seed: int = 1):
+        self.engine = engine
+        self.lib = engine.lib
+        self._h = C.c_void_p()
+        prm = SchedParams(mode, explore_every, probe_rows, train_steps, minibatch, lr,
+                          defer_threshold, fixed_arm, seed)
+        _check(self.lib.gcc_sched_create(engine._h, C.byref(prm), C.byref(self._h)),
+               "gcc_sched_create")
+        self.n_params = int(self.lib.gcc_sched_param_count())
+        self._nb = 0
+
+    def close(self):
+        if self._h:
+            self.lib.gcc_sched_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def run(self, scheme: str, **kw) -> dict:
+        p = self.engine.params(scheme, **kw)
+        r = SchedResult()
+        rc = self.lib.gcc_sched_run(self._h, C.byref(p), C.byref(r))
+        out = {k: getattr(r, k) for k, _ in SchedResult._fields_ if k != "run"}
+        out.update(r.run.as_dict())
+        self.last_result = out
+        n = self.engine.n_tx
+        self._nb = (n + p.batch_size - 1) // p.batch_size
+        self.engine.n_tx = n
+        _check(rc, f"gcc_sched_run({scheme}) err_site={r.run.err_site}")
+        return out
+
+    def batches(self) -> list[dict]:
+        arr = (SchedBatch * self._nb)()
+        _check(self.lib.gcc_sched_batches(self._h, arr, self._nb), "gcc_sched_batches")
+        return [{k: getattr(b, k) for k, _ in SchedBatch._fields_} for b in arr]
+
+    def features(self, first: int, n: int) -> np.ndarray:
+        out = np.zeros((n, SCHED_FEAT_STRIDE), dtype=np.uint16)
+        _check(self.lib.gcc_sched_features(self._h, first, n, _ptr(out)), "gcc_sched_features")
+        return out
+
+    def observe(self, first: int, n: int, clear: bool = False):
+        _check(self.lib.gcc_sched_observe(self._h, first, n, 1 if clear else 0), "gcc_sched_observe")
+
+    def set_weights(self, w: np.ndarray):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        _check(self.lib.gcc_sched_set_weights(self._h, _ptr(w), len(w)), "gcc_sched_set_weights")
+
+    def get_weights(self) -> np.ndarray:
+        w = np.zeros(self.n_params, dtype=np.float32)
+        _check(self.lib.gcc_sched_get_weights(self._h, _ptr(w), len(w)), "gcc_sched_get_weights")
+        return w
+
+    def predict(self, feat: np.ndarray) -> np.ndarray:
+        feat = np.ascontiguousarray(feat, dtype=np.uint16)
+        p = np.zeros(len(feat), dtype=np.float32)
+        _check(self.lib.gcc_sched_predict(self._h, _ptr(feat), len(feat), _ptr(p)), "gcc_sched_predict")
+        return p
+
+    def gradient(self, feat: np.ndarray, labels: np.ndarray):
+        feat = np.ascontiguousarray(feat, dtype=np.uint16)
+        y = np.ascontiguousarray(labels, dtype=np.uint8)
+        g = np.zeros(self.n_params, dtype=np.float32)
+        loss = C.c_double()
+        _check(self.lib.gcc_sched_gradient(self._h, _ptr(feat), _ptr(y), len(feat), _ptr(g),
+                                           C.byref(loss)), "gcc_sched_gradient")
+        return g, loss.value
+
+    def train(self, feat: np.ndarray, labels: np.ndarray, steps: int) -> float:
+        feat = np.ascontiguousarray(feat, dtype=np.uint16)
+        y = np.ascontiguousarray(labels, dtype=np.uint8)
+        loss = C.c_double()
+        _check(self.lib.gcc_sched_train(self._h, _ptr(feat), _ptr(y), len(feat), steps,
+                                        C.byref(loss)), "gcc_sched_train")
+        return loss.value

@@ -22,6 +22,7 @@
 
 #include "cc_launch.cuh"
 #include "prep_kernels.cuh"
+#include "sched.cuh"
 
 using namespace gcc;
 
@@ -1289,6 +1290,594 @@ int gcc_last_kernel_ms(gcc_engine *e, double *kernel_ms, uint64_t *launches) {
     if (!e->have_run) return GCC_ESTATE;
     *kernel_ms = e->last_kernel_ms;
     *launches = e->last_launches;
+    return GCC_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Learned contention scheduling (gcc_sched_*): the per-batch driver around
+// the predictor of sched.cu. Each batch: features -> forward -> stable
+// partition by predicted risk (device) -> policy choice (host, per
+// contention bucket) -> one launch (plain ordering) or two (predicted-safe
+// transactions at full concurrency, then the deferred ones with a cap on
+// transactions in flight) -> the batch's requests enter the frequency table.
+// Every explore_every-th batch first runs a probe of probe_rows transactions
+// with plain ordering at full concurrency: their abort outcomes are the
+// training labels (Adam steps follow) and their abort rate the yardstick.
+// ===========================================================================
+namespace {
+
+struct SchedArm {
+    uint32_t cap;      // in-flight cap of the deferred sub-batch (0: none)
+    uint32_t wd;       // 1: deferred sub-batch under 2PL wait-die
+    uint32_t defer;    // 0: plain ordering, one launch
+};
+
+constexpr int kSchedBuckets = 4;
+
+// Contention bucket of a batch from its mean predicted abort probability.
+int contention_bucket(double pm) {
+    return std::max(0, std::min(kSchedBuckets - 1, (int)(pm * kSchedBuckets)));
+}
+
+}  // namespace
+
+struct gcc_sched {
+    gcc_engine *e = nullptr;
+    gcc_sched_params prm{};
+    sched::Predictor pred;
+    uint32_t *order = nullptr;
+    uint64_t order_cap = 0;
+    uint32_t *part_scratch = nullptr;
+    uint64_t part_cap = 0;
+    uint32_t *counts = nullptr;
+    float *sums = nullptr;
+    std::vector<gcc_sched_batch> batches;
+    // Policy: the arms of the scheme (0 = plain ordering, then deferral with
+    // in-flight caps 2048 / 1024 / 512 / 256, then for 2PL wait-die at 1024
+    // and 512), an incumbent arm, and the arms compared with it since the
+    // last refresh. A refresh happens when the mean prediction of a batch
+    // has moved by more than 0.1 since the previous refresh (the contention
+    // changed) or after 16 batches.
+    std::vector<SchedArm> arms;
+    int policy_scheme = -1;
+    int inc = 0;
+    std::vector<uint8_t> tried;
+    uint32_t since_refresh = 0;
+    float ref_pred = -1.f;
+    ~gcc_sched() {
+        if (e) cudaSetDevice(e->dev);
+        void *bufs[] = {order, part_scratch, counts, sums};
+        for (void *b : bufs)
+            if (b) cudaFree(b);
+    }
+    int fail(cudaError_t ce) {
+        cudaGetLastError();
+        return e->fail_cuda(ce);
+    }
+    void set_arms(int s) {
+        arms.clear();
+        arms.push_back({0u, 0u, 0u});
+        for (uint32_t c : {2048u, 1024u, 512u, 256u}) arms.push_back({c, 0u, 1u});
+        if (s == S_TPL_NW || s == S_TPL_WD)
+            for (uint32_t c : {1024u, 512u}) arms.push_back({c, 1u, 1u});
+        inc = 0;
+        tried.assign(arms.size(), 0);
+        since_refresh = 0;
+        ref_pred = -1.f;
+        policy_scheme = s;
+    }
+    // Candidate to compare against the incumbent for a batch whose mean
+    // prediction is pm, or -1: the next larger or smaller cap (plain ordering
+    // counts as the largest), then the wait-die arm at the incumbent's cap.
+    int candidate(float pm) {
+        if (++since_refresh > 16 || std::fabs(pm - ref_pred) > 0.1f) {
+            std::fill(tried.begin(), tried.end(), 0);
+            since_refresh = 0;
+            ref_pred = pm;
+        }
+        const SchedArm &a = arms[inc];
+        auto plain_cap_arm = [&](uint32_t cap) -> int {
+            for (int k = 0; k < (int)arms.size(); ++k)
+                if (!arms[k].wd && (arms[k].defer ? arms[k].cap : 0u) == cap) return k;
+            return -1;
+        };
+        static const uint32_t kCaps[] = {0u, 2048u, 1024u, 512u, 256u};
+        int r = 0;
+        const uint32_t mycap = a.defer ? a.cap : 0u;
+        while (r < 5 && kCaps[r] != mycap) ++r;
+        for (int nr : {r + 1, r - 1}) {
+            if (nr < 0 || nr >= 5) continue;
+            const int k = plain_cap_arm(kCaps[nr]);
+            if (k >= 0 && k != inc && !tried[k]) return k;
+        }
+        for (int k = 0; k < (int)arms.size(); ++k)
+            if (arms[k].wd != a.wd && arms[k].cap == mycap && arms[k].defer && k != inc && !tried[k])
+                return k;
+        return -1;
+    }
+};
+
+extern "C" {
+
+uint64_t gcc_sched_param_count(void) { return (uint64_t)sched::kParams; }
+
+int gcc_sched_create(gcc_engine *e, const gcc_sched_params *p, gcc_sched **out) {
+    cudaGetLastError();
+    if (!e || !p || !out) return GCC_EINVAL;
+    *out = nullptr;
+    if (p->mode != GCC_SCHED_PLAIN && p->mode != GCC_SCHED_LEARNED) return GCC_EINVAL;
+    if (p->explore_every < 0 || p->minibatch < 0 || p->train_steps < -1 || p->probe_rows < 0 ||
+        p->fixed_arm < 0)
+        return GCC_EINVAL;
+    if (p->minibatch > (1 << 20) || p->probe_rows > (1 << 20)) return GCC_EINVAL;
+    if (!(p->lr >= 0.f) || !(p->defer_threshold >= 0.f) || p->defer_threshold >= 1.f)
+        return GCC_EINVAL;
+    cudaSetDevice(e->dev);
+    gcc_sched *s = new gcc_sched();
+    s->e = e;
+    s->prm = *p;
+    if (!s->prm.explore_every) s->prm.explore_every = 4;
+    if (!s->prm.train_steps) s->prm.train_steps = 4;
+    if (!s->prm.minibatch) s->prm.minibatch = 4096;
+    if (!s->prm.probe_rows) s->prm.probe_rows = 4096;
+    if (s->prm.lr == 0.f) s->prm.lr = 2e-3f;
+    if (s->prm.defer_threshold == 0.f) s->prm.defer_threshold = 0.2f;
+    cudaError_t ce = s->pred.init(e->dev, e->stream,
+                                  (uint64_t)std::max(4096, std::max(s->prm.minibatch, s->prm.probe_rows)),
+                                  p->seed);
+    if (ce == cudaSuccess) ce = cudaMalloc(&s->counts, 16);
+    if (ce == cudaSuccess) ce = cudaMalloc(&s->sums, 16);
+    if (ce != cudaSuccess) {
+        int rc = s->fail(ce);
+        delete s;
+        return ce == cudaErrorMemoryAllocation ? GCC_ENOMEM : rc;
+    }
+    *out = s;
+    return GCC_OK;
+}
+
+void gcc_sched_destroy(gcc_sched *s) { delete s; }
+
+int gcc_sched_set_weights(gcc_sched *s, const float *w, uint64_t n) {
+    if (!s || !w || n != (uint64_t)sched::kParams) return GCC_EINVAL;
+    cudaSetDevice(s->e->dev);
+    cudaError_t ce = s->pred.set_weights(w);
+    return ce == cudaSuccess ? GCC_OK : s->fail(ce);
+}
+
+int gcc_sched_get_weights(gcc_sched *s, float *w, uint64_t n) {
+    if (!s || !w || n != (uint64_t)sched::kParams) return GCC_EINVAL;
+    cudaSetDevice(s->e->dev);
+    cudaError_t ce = s->pred.get_weights(w);
+    return ce == cudaSuccess ? GCC_OK : s->fail(ce);
+}
+
+int gcc_sched_features(gcc_sched *s, uint64_t first, uint64_t n, uint16_t *dst) {
+    if (!s || (!dst && n) || n > (1ull << 20)) return GCC_EINVAL;
+    gcc_engine *e = s->e;
+    if (!e->txs || first + n > e->n_rec) return GCC_ESTATE;
+    cudaSetDevice(e->dev);
+    cudaError_t ce = s->pred.reserve(n);
+    if (ce == cudaSuccess) ce = s->pred.features(e->txs, first, n, s->pred.feat);
+    if (ce == cudaSuccess && n)
+        ce = cudaMemcpyAsync(dst, s->pred.feat, n * sched::kFeatStride * 2, cudaMemcpyDeviceToHost,
+                             e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    return ce == cudaSuccess ? GCC_OK : s->fail(ce);
+}
+
+int gcc_sched_observe(gcc_sched *s, uint64_t first, uint64_t n, int32_t clear) {
+    if (!s) return GCC_EINVAL;
+    gcc_engine *e = s->e;
+    if (n && (!e->txs || first + n > e->n_rec)) return GCC_ESTATE;
+    cudaSetDevice(e->dev);
+    cudaError_t ce = clear ? s->pred.clear_freq() : cudaSuccess;
+    if (ce == cudaSuccess) ce = s->pred.observe(e->txs, first, n);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    return ce == cudaSuccess ? GCC_OK : s->fail(ce);
+}
+
+int gcc_sched_predict(gcc_sched *s, const uint16_t *feat, uint64_t n, float *p) {
+    if (!s || !feat || !p || n == 0 || n > (1ull << 20)) return GCC_EINVAL;
+    gcc_engine *e = s->e;
+    cudaSetDevice(e->dev);
+    cudaError_t ce = s->pred.reserve(n);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(s->pred.feat, feat, n * sched::kFeatStride * 2, cudaMemcpyHostToDevice,
+                             e->stream);
+    if (ce == cudaSuccess) ce = s->pred.forward(s->pred.feat, n, s->pred.p);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(p, s->pred.p, n * 4, cudaMemcpyDeviceToHost, e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    return ce == cudaSuccess ? GCC_OK : s->fail(ce);
+}
+
+static int sched_upload_rows(gcc_sched *s, const uint16_t *feat, const uint8_t *labels,
+                             uint64_t n) {
+    gcc_engine *e = s->e;
+    cudaError_t ce = s->pred.reserve(n);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(s->pred.feat, feat, n * sched::kFeatStride * 2, cudaMemcpyHostToDevice,
+                             e->stream);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(s->pred.labels, labels, n, cudaMemcpyHostToDevice, e->stream);
+    return ce == cudaSuccess ? GCC_OK : s->fail(ce);
+}
+
+int gcc_sched_gradient(gcc_sched *s, const uint16_t *feat, const uint8_t *labels, uint64_t n,
+                       float *grad, double *loss) {
+    if (!s || !feat || !labels || !grad || n == 0 || n > (1ull << 20)) return GCC_EINVAL;
+    gcc_engine *e = s->e;
+    cudaSetDevice(e->dev);
+    int rc = sched_upload_rows(s, feat, labels, n);
+    if (rc) return rc;
+    float lsum = 0.f;
+    cudaError_t ce = s->pred.gradient(s->pred.feat, s->pred.labels, n);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(grad, s->pred.grad, sched::kParams * 4, cudaMemcpyDeviceToHost, e->stream);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(&lsum, s->pred.loss, 4, cudaMemcpyDeviceToHost, e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    if (ce != cudaSuccess) return s->fail(ce);
+    if (loss) *loss = (double)lsum / (double)n;
+    return GCC_OK;
+}
+
+int gcc_sched_train(gcc_sched *s, const uint16_t *feat, const uint8_t *labels, uint64_t n,
+                    int32_t steps, double *loss) {
+    if (!s || !feat || !labels || n == 0 || n > (1ull << 20) || steps < 1) return GCC_EINVAL;
+    gcc_engine *e = s->e;
+    cudaSetDevice(e->dev);
+    int rc = sched_upload_rows(s, feat, labels, n);
+    if (rc) return rc;
+    const uint64_t mb = std::min<uint64_t>(n, (uint64_t)s->prm.minibatch);
+    cudaError_t ce = cudaSuccess;
+    float lsum = 0.f;
+    uint64_t rows = mb;
+    for (int32_t k = 0; k < steps && ce == cudaSuccess; ++k) {
+        const uint64_t off = ((uint64_t)k * mb) % n;
+        rows = std::min<uint64_t>(mb, n - off);
+        ce = s->pred.gradient(s->pred.feat + off * sched::kFeatStride, s->pred.labels + off, rows);
+        if (ce == cudaSuccess) ce = s->pred.adam(s->prm.lr);
+    }
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(&lsum, s->pred.loss, 4, cudaMemcpyDeviceToHost, e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    if (ce != cudaSuccess) return s->fail(ce);
+    if (loss) *loss = (double)lsum / (double)rows;
+    return GCC_OK;
+}
+
+int gcc_sched_batches(gcc_sched *s, gcc_sched_batch *dst, uint64_t n) {
+    if (!s || (!dst && n)) return GCC_EINVAL;
+    if (n > s->batches.size()) return GCC_ESTATE;
+    for (uint64_t i = 0; i < n; ++i) dst[i] = s->batches[i];
+    return GCC_OK;
+}
+
+int gcc_sched_run(gcc_sched *sc, const gcc_run_params *rp, gcc_sched_result *out) {
+    cudaGetLastError();
+    if (!sc || !rp || !out) return GCC_EINVAL;
+    memset(out, 0, sizeof(*out));
+    gcc_engine *e = sc->e;
+    const int s = gcc_scheme_id(rp->cc_scheme);
+    if (s != S_TPL_NW && s != S_TPL_WD && s != S_SILO && s != S_TICTOC) return GCC_EINVAL;
+    if (rp->warp_density < 0 || rp->warp_density > 5) return GCC_EINVAL;
+    if (rp->block_size < 1 || rp->block_size > 32) return GCC_EINVAL;
+    if (rp->batch_size < 1 || rp->batch_size > (1 << 20)) return GCC_EINVAL;
+    if (rp->write_mode != GCC_WRITE_FIELD) return GCC_EINVAL;
+    if (rp->flags & (GCC_F_READ_LOG | GCC_F_AUTOTUNE | GCC_F_GRAPH)) return GCC_EINVAL;
+    if (rp->backoff_ns < -1 || rp->backoff_ns > 100000) return GCC_EINVAL;
+    if (rp->max_active < 0 || rp->starve_limit < -1) return GCC_EINVAL;
+    if (!e->txs || e->n_rec == 0) return GCC_ESTATE;
+    cudaSetDevice(e->dev);
+    e->n_tx = e->n_rec;
+    const bool learned = sc->prm.mode == GCC_SCHED_LEARNED;
+    const uint64_t n = e->n_tx;
+    const uint64_t batch = std::min<uint64_t>((uint64_t)rp->batch_size, n);
+    const uint64_t nb = (n + batch - 1) / batch;
+    const int G = 1 << rp->warp_density, block = rp->block_size * 32;
+    int rc;
+    cudaError_t ce;
+    if ((ce = sc->pred.reserve(batch))) return sc->fail(ce);
+    if (sc->order_cap < n) {
+        if (sc->order) cudaFree(sc->order);
+        sc->order = nullptr;
+        if ((ce = cudaMalloc(&sc->order, n * 4))) return sc->fail(ce);
+        sc->order_cap = n;
+    }
+    const uint64_t pneed = (batch + 1023) / 1024 * 3;
+    if (sc->part_cap < pneed) {
+        if (sc->part_scratch) cudaFree(sc->part_scratch);
+        sc->part_scratch = nullptr;
+        if ((ce = cudaMalloc(&sc->part_scratch, pneed * 4))) return sc->fail(ce);
+        sc->part_cap = pneed;
+    }
+    const int occ_main = scheme_occupancy(s, G, block);
+    const int occ_wd = scheme_occupancy(S_TPL_WD, G, block);
+    if (occ_main <= 0 || occ_wd <= 0) return GCC_EINVAL;
+    if (sc->policy_scheme != s) sc->set_arms(s);
+
+    KParams base = e->base_params();
+    base.write_mode = rp->write_mode;
+    base.write_seed = rp->write_seed;
+    base.flags = rp->flags;
+    base.spin_limit_ns = rp->spin_limit_ns ? rp->spin_limit_ns : 4000000000ull;
+    base.backoff_ns = rp->backoff_ns < 0 ? 0u : (rp->backoff_ns == 0 ? 512u : (uint32_t)rp->backoff_ns);
+    base.starve_limit = starve_param(rp->starve_limit);
+    const uint64_t user_grid = std::min<uint64_t>((uint64_t)occ_main * e->sm_count,
+                                                  active_grid(rp->max_active, G, block));
+
+    if ((rc = e->ensure_events(8))) return rc;
+    cudaEvent_t ev0 = e->events[0], ev1 = e->events[1], evk0 = e->events[2], evk1 = e->events[3],
+                evt0 = e->events[4], evt1 = e->events[5], evp1 = e->events[6], evq = e->events[7];
+    cudaStream_t st = e->stream;
+    if ((ce = cudaMemsetAsync(e->ctr, 0, sizeof(Counters), st))) return sc->fail(ce);
+    sc->batches.assign(nb, gcc_sched_batch{});
+    const uint64_t launches0 = e->kernel_launches;
+    double tot_ms = 0, proc_ms = 0, pred_ms = 0, train_ms = 0, probe_ms = 0, sched_ms = 0;
+    uint64_t probe_c = 0, probe_a = 0, sched_c = 0, sched_a = 0;
+    unsigned long long prev[2] = {0, 0};
+    std::vector<uint8_t> ylab;
+
+    auto launch = [&](int sch, uint64_t bst, uint64_t bn, const uint32_t *order,
+                      uint64_t grid_cap) -> cudaError_t {
+        KParams q = base;
+        q.batch_st = (uint32_t)bst;
+        q.batch_n = (uint32_t)bn;
+        q.order = order;
+        q.wait_die = sch == S_TPL_WD ? 1u : 0u;
+        k_batch_prep<<<1, 32, 0, st>>>(e->ctr, 0);
+        cudaError_t c = cudaGetLastError();
+        if (c != cudaSuccess) return c;
+        const uint64_t want = (bn * (uint64_t)G + block - 1) / block;
+        const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, grid_cap));
+        e->kernel_launches += 2;
+        return launch_scheme_kernel(sch, G, grid, block, q, st);
+    };
+    auto counters = [&](unsigned long long *ca) -> cudaError_t {
+        cudaError_t c = cudaMemcpyAsync(ca, &e->ctr->committed, 16, cudaMemcpyDeviceToHost, st);
+        return c == cudaSuccess ? cudaStreamSynchronize(st) : c;
+    };
+
+    // one part of a batch under an arm: plain ordering (one launch), or the
+    // predicted-safe transactions at full concurrency then the deferred ones
+    // with the arm's in-flight cap
+    auto run_part = [&](const SchedArm &a, uint64_t st0, uint64_t cnt, uint32_t n_low) -> cudaError_t {
+        if (!cnt) return cudaSuccess;
+        if (!a.defer) return launch(s, st0, cnt, nullptr, user_grid);
+        cudaError_t c = cudaSuccess;
+        if (n_low) c = launch(s, st0, n_low, sc->order, user_grid);
+        if (c == cudaSuccess && cnt > n_low) {
+            const int sch2 = a.wd ? S_TPL_WD : s;
+            const int occ2 = a.wd ? occ_wd : occ_main;
+            const uint64_t cap_grid = std::min<uint64_t>((uint64_t)occ2 * e->sm_count,
+                                                         active_grid((int32_t)a.cap, G, block));
+            c = launch(sch2, st0 + n_low, cnt - n_low, sc->order, cap_grid);
+        }
+        return c;
+    };
+
+    for (uint64_t b = 0; b < nb; ++b) {
+        const uint64_t bst = b * batch, bn = std::min<uint64_t>(batch, n - bst);
+        gcc_sched_batch &rec = sc->batches[b];
+        const uint64_t probe = (learned && b % (uint64_t)sc->prm.explore_every == 0)
+                                   ? std::min<uint64_t>(bn, (uint64_t)sc->prm.probe_rows) : 0;
+        const uint64_t rst = bst + probe, rn = bn - probe;
+        rec.kind = learned ? 1u : 0u;
+        rec.probe = (uint32_t)probe;
+        if ((ce = cudaEventRecord(ev0, st))) return sc->fail(ce);
+        if (b == 0 || !(rp->flags & GCC_F_NO_RESET))
+            if ((ce = cudaMemsetAsync(e->meta, 0, e->rows * 8, st))) return sc->fail(ce);
+        // the part after the probe runs under the bucket's incumbent arm; when
+        // the bucket has a candidate, its second half runs under the
+        // candidate instead, so both arms meet the same workload
+        int arm_i = 0, cand = -1;
+        uint64_t seg_n[2] = {rn, 0};
+        uint32_t n_low[2] = {(uint32_t)rn, 0};
+        float bpred_ms = 0;
+        if (learned) {
+            ce = sc->pred.features(e->txs, bst, bn, sc->pred.feat);
+            if (ce == cudaSuccess) ce = sc->pred.forward(sc->pred.feat, bn, sc->pred.p);
+            e->kernel_launches += 4;  // features, 2 GEMMs + head
+            // the bucket comes from the mean prediction over the batch
+            float hsums[4] = {0.f, 0.f, 0.f, 0.f};
+            if (ce == cudaSuccess) {
+                ce = sched::partition(sc->pred.p, bst, bn, sc->prm.defer_threshold, sc->order + bst,
+                                      sc->counts, sc->sums, sc->part_scratch, st);
+                e->kernel_launches += 3;
+            }
+            if (ce == cudaSuccess) ce = cudaMemcpyAsync(hsums, sc->sums, 8, cudaMemcpyDeviceToHost, st);
+            if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+            if (ce != cudaSuccess) return sc->fail(ce);
+            rec.pred_mean = hsums[0] / (float)bn;
+            rec.bucket = (uint32_t)contention_bucket(rec.pred_mean);
+            if (sc->prm.fixed_arm > 0) {
+                arm_i = std::min<int>(sc->prm.fixed_arm - 1, (int)sc->arms.size() - 1);
+            } else {
+                arm_i = sc->inc;
+                cand = rn >= 2048 ? sc->candidate(rec.pred_mean) : -1;
+            }
+            if (cand >= 0) {
+                seg_n[0] = rn / 2;
+                seg_n[1] = rn - seg_n[0];
+            }
+            // risk partition of each part (positions keep their part)
+            uint64_t off = rst;
+            for (int k = 0; k < 2 && ce == cudaSuccess; ++k) {
+                if (!seg_n[k]) continue;
+                ce = sched::partition(sc->pred.p + (off - bst), off, seg_n[k], sc->prm.defer_threshold,
+                                      sc->order + off, sc->counts + k, sc->sums + 2 * k,
+                                      sc->part_scratch, st);
+                e->kernel_launches += 3;
+                off += seg_n[k];
+            }
+            if (ce == cudaSuccess) ce = cudaMemcpyAsync(n_low, sc->counts, 8, cudaMemcpyDeviceToHost, st);
+            if (ce == cudaSuccess) ce = cudaEventRecord(evp1, st);
+            if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+            if (ce != cudaSuccess) return sc->fail(ce);
+            if (!seg_n[1]) n_low[1] = 0;
+            cudaEventElapsedTime(&bpred_ms, ev0, evp1);
+            pred_ms += bpred_ms;
+        }
+        const SchedArm arm = sc->arms[arm_i];
+        rec.arm = (uint32_t)arm_i;
+        rec.explored = cand >= 0 ? (uint32_t)cand + 1u : 0u;
+        rec.in_flight_cap = arm.defer ? arm.cap : 0u;
+        rec.wait_die = arm.defer ? arm.wd : 0u;
+        rec.deferred = (arm.defer ? seg_n[0] - n_low[0] : 0u) +
+                       (cand >= 0 && sc->arms[cand].defer ? seg_n[1] - n_low[1] : 0u);
+
+        // the probe: plain ordering at full concurrency, labels for training
+        unsigned long long c_probe[2] = {prev[0], prev[1]};
+        if (probe) {
+            if ((ce = launch(s, bst, probe, nullptr, user_grid))) return sc->fail(ce);
+            if ((ce = cudaEventRecord(evq, st))) return sc->fail(ce);
+            if ((ce = counters(c_probe))) return sc->fail(ce);
+            float qms = 0;
+            cudaEventElapsedTime(&qms, learned ? evp1 : ev0, evq);
+            probe_ms += qms;
+            probe_c += c_probe[0] - prev[0];
+            probe_a += c_probe[1] - prev[1];
+        }
+        if ((ce = cudaEventRecord(evk0, st))) return sc->fail(ce);
+        ce = run_part(arm, rst, seg_n[0], n_low[0]);
+        if (ce == cudaSuccess) ce = cudaEventRecord(evt1, st);  // end of the first part
+        if (ce == cudaSuccess && cand >= 0) ce = run_part(sc->arms[cand], rst + seg_n[0], seg_n[1], n_low[1]);
+        if (ce == cudaSuccess) ce = cudaEventRecord(evk1, st);
+        if (ce != cudaSuccess) return sc->fail(ce);
+        float part_ms[2] = {0.f, 0.f};
+        if (cand >= 0) {
+            if ((ce = cudaEventSynchronize(evk1))) return sc->fail(ce);
+            cudaEventElapsedTime(&part_ms[0], evk0, evt1);
+            cudaEventElapsedTime(&part_ms[1], evt1, evk1);
+        }
+
+        if (probe && sc->prm.train_steps > 0) {
+            // labels of the probe, the loss of the predictions made before
+            // training on them, then Adam steps
+            ce = cudaEventRecord(evt0, st);
+            if (ce == cudaSuccess) ce = sched::abort_labels(e->tx_aborts, bst, probe, sc->pred.labels, st);
+            e->kernel_launches += 1;
+            ylab.resize(probe);
+            if (ce == cudaSuccess)
+                ce = cudaMemcpyAsync(ylab.data(), sc->pred.labels, probe, cudaMemcpyDeviceToHost, st);
+            const uint64_t mb = std::min<uint64_t>(probe, (uint64_t)sc->prm.minibatch);
+            for (int32_t k = 0; k < sc->prm.train_steps && ce == cudaSuccess; ++k) {
+                const uint64_t off = ((uint64_t)k * mb) % probe;
+                const uint64_t rows = std::min<uint64_t>(mb, probe - off);
+                ce = sc->pred.gradient(sc->pred.feat + off * sched::kFeatStride,
+                                       sc->pred.labels + off, rows);
+                if (ce == cudaSuccess && k == 0) {
+                    float l0 = 0.f;
+                    ce = cudaMemcpyAsync(&l0, sc->pred.loss, 4, cudaMemcpyDeviceToHost, st);
+                    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+                    rec.loss = l0 / (float)rows;
+                }
+                if (ce == cudaSuccess) ce = sc->pred.adam(sc->prm.lr);
+                e->kernel_launches += 13;
+            }
+            if (ce == cudaSuccess) ce = cudaEventRecord(evt1, st);
+            if (ce != cudaSuccess) return sc->fail(ce);
+        }
+        if (learned) {
+            if ((ce = sc->pred.observe(e->txs, bst, bn))) return sc->fail(ce);
+            e->kernel_launches += 2;
+        }
+        if ((ce = cudaEventRecord(ev1, st))) return sc->fail(ce);
+        unsigned long long ca[2];
+        if ((ce = counters(ca))) return sc->fail(ce);
+        float ms = 0, kms = 0;
+        cudaEventElapsedTime(&ms, ev0, ev1);
+        cudaEventElapsedTime(&kms, evk0, evk1);
+        if (probe && sc->prm.train_steps > 0) {
+            float tms = 0;
+            cudaEventElapsedTime(&tms, evt0, evt1);
+            train_ms += tms;
+            uint64_t pos = 0;
+            for (uint8_t v : ylab) pos += v;
+            rec.label_mean = (float)pos / (float)probe;
+        }
+        rec.ms = ms;
+        rec.committed = ca[0] - prev[0];
+        rec.aborts = ca[1] - prev[1];
+        tot_ms += ms;
+        proc_ms += kms;
+        sched_ms += kms;
+        sched_c += ca[0] - c_probe[0];
+        sched_a += ca[1] - c_probe[1];
+        prev[0] = ca[0];
+        prev[1] = ca[1];
+        // the comparison: the candidate replaces the incumbent when its half
+        // ran at least 3% faster per transaction
+        if (cand >= 0) {
+            sc->tried[cand] = 1;
+            const double t_inc = part_ms[0] / (double)seg_n[0];
+            const double t_cand = part_ms[1] / (double)seg_n[1];
+            if (t_cand < 0.97 * t_inc) {
+                sc->tried[arm_i] = 1;
+                sc->inc = cand;
+            }
+        }
+        unsigned err = 0;
+        if (cudaMemcpy(&err, &e->ctr->err, 4, cudaMemcpyDeviceToHost) == cudaSuccess && err) break;
+    }
+
+    Counters hc;
+    ce = cudaMemcpy(&hc, e->ctr, sizeof(Counters), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return sc->fail(ce);
+    e->have_run = true;
+    e->last_kernel_ms = proc_ms;
+    e->last_launches = nb;
+    gcc_result *r = &out->run;
+    r->committed = hc.committed;
+    r->aborts = hc.aborts;
+    r->pre_s = (pred_ms + train_ms) / 1000.0;
+    r->proc_s = (proc_ms + probe_ms) / 1000.0;
+    r->tot_s = tot_ms / 1000.0;
+    r->tx_per_s = tot_ms > 0 ? (double)hc.committed * 1000.0 / tot_ms : 0.0;
+    const double inv = 1.0 / ((double)n * (double)e->clock_khz);
+    r->ts_d = hc.ts_cycles * inv;
+    r->wait_d = hc.wait_cycles * inv;
+    r->abort_d = hc.abort_cycles * inv;
+    r->mng_d = hc.mng_cycles * inv;
+    r->tot_d = hc.tot_cycles * inv;
+    r->idx_d = hc.idx_cycles * inv;
+    r->batches = nb;
+    r->kernel_launches = e->kernel_launches - launches0;
+    r->max_attempts = hc.max_attempts;
+    r->err_site = hc.err_where;
+    uint64_t total = 0;
+    for (int i = 0; i < kHistBuckets; ++i) total += hc.hist[i];
+    auto edge = [](int bk) -> double {
+        if (bk < 16) return (double)bk + 1.0;
+        int lg = bk / 16 + 3, sub = bk % 16;
+        return std::ldexp(16.0 + sub + 1.0, lg - 4);
+    };
+    auto pct = [&](double q) -> double {
+        if (!total) return 0.0;
+        uint64_t target = (uint64_t)std::ceil(q * (double)total), acc = 0;
+        for (int i = 0; i < kHistBuckets; ++i) {
+            acc += hc.hist[i];
+            if (acc >= target) return edge(i) / 1000.0;
+        }
+        return edge(kHistBuckets - 1) / 1000.0;
+    };
+    r->lat_p50_us = pct(0.50);
+    r->lat_p99_us = pct(0.99);
+    for (auto &rec : sc->batches) {
+        out->probed += rec.probe;
+        out->deferred += rec.deferred;
+        if (rec.probe && sc->prm.train_steps > 0) out->last_loss = rec.loss;
+    }
+    out->probe_tx_per_s = probe_ms > 0 ? probe_c * 1000.0 / probe_ms : 0.0;
+    out->sched_tx_per_s = sched_ms > 0 ? sched_c * 1000.0 / sched_ms : 0.0;
+    out->probe_abort_rate = probe_c + probe_a ? (double)probe_a / (double)(probe_c + probe_a) : 0.0;
+    out->sched_abort_rate = sched_c + sched_a ? (double)sched_a / (double)(sched_c + sched_a) : 0.0;
+    out->predict_ms = pred_ms;
+    out->train_ms = train_ms;
+    if (hc.err) return (int)hc.err;
+    if (hc.committed != n) return GCC_ESTATE;
     return GCC_OK;
 }
 

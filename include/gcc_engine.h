@@ -288,6 +288,107 @@ int gcc_run_tpl_nw_noalloc(const gcc_ycsb_tx *txs, uint64_t n_tx, void *table,
  * launches of the transaction kernel (for roofline accounting). */
 int gcc_last_kernel_ms(gcc_engine *e, double *kernel_ms, uint64_t *launches);
 
+/* ---- Learned contention scheduling (no counterpart in the reference,
+ * which runs every batch in transaction-index order with one launch,
+ * benchmark_cpu/ycsb.cu:262-285). A small MLP (66 -> 128 -> 128 -> 1, BF16
+ * weights, FP32 accumulation, sigmoid) predicts per transaction the
+ * probability that it aborts at least once under plain ordering. Each
+ * scheduled batch runs its predicted-safe transactions first at full
+ * concurrency and defers the rest into a second sub-batch with a cap on
+ * transactions in flight (and, for 2PL, no-wait or wait-die). The choice is
+ * measured, with plain ordering as one of the choices: a batch runs its
+ * first half under the incumbent choice and its second half under a
+ * neighbouring one, and the faster becomes the incumbent; the comparisons
+ * restart when the network's mean prediction shows the contention moved. Every explore_every-th batch first runs a probe of probe_rows
+ * transactions with plain ordering at full concurrency: their abort outcomes
+ * are the training labels (Adam on the GPU) and their abort rate the
+ * yardstick. CC arithmetic and commit rules are untouched. Schemes: tpl_nw,
+ * tpl_wd, silo, tictoc; 16-request records loaded with gcc_load_txs;
+ * batch_size at most 1,048,576. */
+#define GCC_SCHED_PLAIN 0   /* plain ordering every batch (same driver) */
+#define GCC_SCHED_LEARNED 1
+#define GCC_SCHED_FEAT_STRIDE 72 /* u16 per feature row (66 used) */
+
+typedef struct gcc_sched gcc_sched;
+
+typedef struct gcc_sched_params {
+    int32_t mode;            /* GCC_SCHED_* */
+    int32_t explore_every;   /* every n-th batch starts with a probe; 0 = 4 */
+    int32_t probe_rows;      /* transactions of a probe; 0 = 4096 */
+    int32_t train_steps;     /* Adam steps after each probe; 0 = 4, -1 = none */
+    int32_t minibatch;       /* rows per step; 0 = 4096 */
+    float lr;                /* Adam learning rate; 0 = 2e-3 */
+    float defer_threshold;   /* predicted probability above which a
+                                transaction is deferred; 0 = 0.2 */
+    int32_t fixed_arm;       /* 0: the policy chooses; k > 0: every batch
+                                runs arm k-1 of: plain ordering, deferral
+                                with in-flight cap 2048, 1024, 512, 256, and
+                                for 2PL wait-die deferral at 1024, 512 */
+    uint64_t seed;           /* initial weights (He-uniform from this seed) */
+} gcc_sched_params;
+
+typedef struct gcc_sched_batch {
+    uint32_t kind;           /* 0 plain mode, 1 scheduled */
+    uint32_t bucket;         /* contention level: mean prediction x 4 */
+    uint32_t arm;            /* the incumbent arm (0 = plain ordering) */
+    uint32_t in_flight_cap;  /* cap of the deferred sub-batch (0 = none) */
+    uint32_t wait_die;       /* deferred sub-batch ran 2PL wait-die */
+    uint32_t probe;          /* transactions of the batch's probe */
+    uint64_t deferred;       /* transactions in the deferred sub-batch */
+    float pred_mean;         /* mean predicted abort probability (after the probe) */
+    float label_mean;        /* probes: fraction that aborted */
+    float loss;              /* probes: mean BCE of the predictions made
+                                before training on the probe */
+    uint32_t explored;       /* 1 + the arm the batch's second half ran to
+                                compare it with the incumbent (0 = none) */
+    double ms;               /* device time of the batch incl. scheduling */
+    uint64_t committed, aborts;
+} gcc_sched_batch;
+
+typedef struct gcc_sched_result {
+    gcc_result run;          /* totals over all batches, as gcc_run */
+    uint64_t probed, deferred;
+    double probe_tx_per_s;   /* committed / kernel time of the probes */
+    double sched_tx_per_s;   /* the same over the non-probe parts */
+    double probe_abort_rate; /* aborts / (aborts + committed) in probes */
+    double sched_abort_rate; /* the same over the non-probe parts */
+    double predict_ms, train_ms; /* device time of inference / training */
+    double last_loss;        /* BCE of the last probe's predictions */
+} gcc_sched_result;
+
+int gcc_sched_create(gcc_engine *e, const gcc_sched_params *p, gcc_sched **out);
+void gcc_sched_destroy(gcc_sched *s);
+/* Run the loaded records in batches of rp->batch_size under the schedule
+ * (rp->max_active, if set, caps the plain sub-batches too). Synchronous;
+ * the engine's outputs (table, digests, commit log, tx aborts) are those of
+ * the run. The frequency table, weights and policy statistics persist
+ * across runs. */
+int gcc_sched_run(gcc_sched *s, const gcc_run_params *rp, gcc_sched_result *out);
+/* Per-batch records of the last run (n <= its batch count). */
+int gcc_sched_batches(gcc_sched *s, gcc_sched_batch *dst, uint64_t n);
+/* Features of loaded records first .. first+n-1 against the current
+ * frequency table: n rows of GCC_SCHED_FEAT_STRIDE u16 (host). */
+int gcc_sched_features(gcc_sched *s, uint64_t first, uint64_t n, uint16_t *dst);
+/* Count records first .. first+n-1 into the frequency table (after halving
+ * it), as a run does after each batch; clear = 1 zeroes it first. */
+int gcc_sched_observe(gcc_sched *s, uint64_t first, uint64_t n, int32_t clear);
+/* Parameters: gcc_sched_param_count() FP32 values, layout W1[66][128],
+ * b1[128], W2[128][128], b2[128], w3[128], b3. set rounds them to BF16 for
+ * compute and resets Adam. */
+uint64_t gcc_sched_param_count(void);
+int gcc_sched_set_weights(gcc_sched *s, const float *w, uint64_t n);
+int gcc_sched_get_weights(gcc_sched *s, float *w, uint64_t n);
+/* Forward pass over n host feature rows -> p[n] (host). */
+int gcc_sched_predict(gcc_sched *s, const uint16_t *feat, uint64_t n, float *p);
+/* Gradient of the mean binary cross-entropy over n host rows with 0/1
+ * labels -> grad[param_count] (host), *loss = the mean loss. */
+int gcc_sched_gradient(gcc_sched *s, const uint16_t *feat, const uint8_t *labels, uint64_t n,
+                       float *grad, double *loss);
+/* steps Adam steps on minibatches of the given rows (cycling through them);
+ * *loss = mean loss of the last step. */
+int gcc_sched_train(gcc_sched *s, const uint16_t *feat, const uint8_t *labels, uint64_t n,
+                    int32_t steps, double *loss);
+
 #ifdef __cplusplus
 }
 #endif

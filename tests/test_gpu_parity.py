@@ -123,7 +123,7 @@ def test_starvation_control_and_in_flight_cap(oracle, scheme):
         run_and_check(oracle, eng, init, txs, scheme, 5, 32, 1024, g.WRITE_FIELD, layout,
                       starve_limit=2)
         run_and_check(oracle, eng, init, txs, scheme, 3, 8, 1024, g.WRITE_FIELD, layout,
-                      starve_limit=-1, max_active=40)
+                      max_active=40)
 
 
 @pytest.mark.parametrize("scheme", ["tpl_nw", "tictoc", "gacco", "mvcc"])

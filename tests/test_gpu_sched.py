@@ -1,0 +1,159 @@
+"""Learned contention scheduling on the GPU: the predictor's CUDA kernels
+against the numpy oracle (features bit-exact; forward and the gradient of the
+mean BCE within FP32-accumulation tolerance), training that lowers the loss,
+scheduled runs that stay serializable (commit-order replay reproduces the
+table and every read digest), and what the trained network gains over plain
+ordering on a contended workload."""
+import numpy as np
+import pytest
+
+import gpu_cc_tb_b200 as g
+from oracle import predictor as P
+
+pytestmark = pytest.mark.gpu
+SPIN = 2_000_000_000
+
+
+@pytest.fixture(scope="module")
+def eng_small():
+    rows = 100_000
+    txs = g.gen_ycsb(rows, 6000, 0.95, 0.6, seed=23, dedup=g.DEDUP_DROP, key_base=0)
+    eng = g.Engine(rows, layout=g.LAYOUT_U64X11, index=g.INDEX_HASH, fill_seed=3, max_batch=2048)
+    eng.load_txs(txs)
+    yield eng, txs
+    eng.close()
+
+
+def test_param_count():
+    assert g.library().gcc_sched_param_count() == P.N_PARAMS == 25217
+
+
+def test_features_and_frequency_table_bit_exact(eng_small):
+    eng, txs = eng_small
+    with g.Scheduler(eng) as sc:
+        freq = np.zeros(1 << P.FREQ_BITS, dtype=np.uint32)
+        sc.observe(0, 0, clear=True)
+        for first in (0, 2000, 4000):
+            sc.observe(first, 2000)
+            freq = P.observe(freq, txs[first:first + 2000])
+        got = sc.features(0, len(txs))
+        want = P.features(txs, freq)
+        assert (want[:, 65] > 16).any()  # hot keys seen
+        assert np.array_equal(got, want)
+
+
+def test_forward_and_gradient_match_oracle(eng_small):
+    eng, txs = eng_small
+    rng = np.random.default_rng(7)
+    with g.Scheduler(eng, seed=11) as sc:
+        w = sc.get_weights()
+        # the initial weights and a random perturbation of them
+        for trial in range(2):
+            if trial:
+                w = (w + rng.normal(0, 0.05, w.shape)).astype(np.float32)
+                sc.set_weights(w)
+            feat = sc.features(0, 3000)
+            feat[:, 64] = rng.integers(0, 17, 3000)
+            feat[:, 65] = rng.integers(0, 17, 3000)
+            y = rng.integers(0, 2, 3000).astype(np.uint8)
+            p = sc.predict(feat)
+            _, _, _, _, pref = P.forward(w, feat)
+            assert np.max(np.abs(p - pref)) < 2e-5
+            grad, loss = sc.gradient(feat, y)
+            lref, gref = P.loss_and_grad(w, feat, y)
+            assert abs(loss - lref) <= 1e-5 * abs(lref) + 1e-6
+            tol = 1e-4 * np.max(np.abs(gref)) + 1e-7
+            bad = np.abs(grad - gref) > tol
+            assert not bad.any(), (np.nonzero(bad)[0][:8], np.max(np.abs(grad - gref)), tol)
+
+
+def test_training_lowers_loss(eng_small):
+    eng, txs = eng_small
+    with g.Scheduler(eng, seed=5, minibatch=1024, lr=3e-3) as sc:
+        sc.observe(0, 6000, clear=True)
+        feat = sc.features(0, 6000)
+        # a learnable rule on the write count
+        y = (feat[:, 64] > np.median(feat[:, 64])).astype(np.uint8)
+        assert 0.1 < y.mean() < 0.9
+        _, l0 = sc.gradient(feat, y)
+        sc.train(feat, y, 200)
+        _, l1 = sc.gradient(feat, y)
+        acc = ((sc.predict(feat) > 0.5) == (y == 1)).mean()
+        assert l1 < 0.5 * l0 and acc > 0.95, (l0, l1, acc)
+
+
+def _replay_check(oracle, eng, init, txs, seed):
+    table, dg = eng.dump_table(), eng.digests()
+    order = oracle.commit_order(eng.commit_log())
+    assert sorted(order.tolist()) == list(range(len(txs)))
+    ref_t, ref_dg, _ = oracle.replay(init, g.LAYOUT_U64X11, txs, order, g.WRITE_FIELD, seed)
+    assert np.array_equal(table, ref_t)
+    assert np.array_equal(dg, ref_dg)
+
+
+def _write_count_network():
+    # p > 0.5 exactly when a transaction has more than 8 write requests:
+    # z = 8 * relu(writes / 16) - 4
+    w = np.zeros(P.N_PARAMS, dtype=np.float32)
+    w[P.OFF_W1 + 64 * P.N_HID + 0] = 1.0
+    w[P.OFF_W2 + 0 * P.N_HID + 0] = 1.0
+    w[P.OFF_W3 + 0] = 8.0
+    w[P.OFF_B3] = -4.0
+    return w
+
+
+@pytest.mark.parametrize("scheme,arm", [("tpl_nw", 0), ("tpl_nw", 4), ("tpl_wd", 3),
+                                        ("tpl_nw", 7), ("silo", 0), ("silo", 3), ("tictoc", 0),
+                                        ("tictoc", 5)])
+def test_scheduled_runs_are_serializable(oracle, scheme, arm):
+    # arm 0: the policy (probes, in-batch comparisons); arm k > 0: every
+    # batch defers the predicted-risky transactions (more than 8 writes)
+    # into a capped sub-batch of arm k - 1
+    rows = 20_000
+    txs = g.gen_ycsb(rows, 24_576, 0.95, 0.4, seed=41, dedup=g.DEDUP_RESAMPLE, key_base=0)
+    init = oracle.fill_table(rows, g.LAYOUT_U64X11, 8)
+    with g.Engine(rows, layout=g.LAYOUT_U64X11, index=g.INDEX_HASH, fill_seed=8,
+                  max_batch=4096) as eng, \
+            g.Scheduler(eng, explore_every=3, probe_rows=512, train_steps=4 if arm == 0 else -1,
+                        minibatch=512, fixed_arm=arm) as sc:
+        eng.load_txs(txs)
+        if arm:
+            sc.set_weights(_write_count_network())
+        explored = 0
+        for run in range(2):
+            eng.upload_table(init)
+            r = sc.run(scheme, warp_density=5, block_size=32, batch_size=4096,
+                       flags=g.F_COMMIT_LOG, write_seed=31 + run, spin_limit_ns=SPIN)
+            assert r["committed"] == len(txs)
+            assert r["probed"] == 2 * 512
+            _replay_check(oracle, eng, init, txs, 31 + run)
+            explored += sum(1 for b in sc.batches() if b["explored"])
+        recs = sc.batches()
+        assert all(b["kind"] == 1 and b["committed"] > 0 for b in recs)
+        if arm:
+            feat = sc.features(0, len(txs))
+            risky = int((feat[:, 64] > 8).sum())
+            assert 0 < sum(b["deferred"] for b in recs) <= risky
+        else:
+            assert explored > 0
+
+
+def test_trained_network_beats_plain_ordering(oracle):
+    # contended YCSB: theta 0.99 on 1,048,576 rows, 16 batches of 16,384
+    rows, nb, bsz = 1_048_576, 16, 16_384
+    txs = g.gen_ycsb(rows, nb * bsz, 0.99, 0.5, seed=77, dedup=g.DEDUP_RESAMPLE, key_base=0)
+    with g.Engine(rows, layout=g.LAYOUT_U64X11, index=g.INDEX_HASH, fill_seed=1,
+                  max_batch=bsz) as eng:
+        eng.load_txs(txs)
+        kw = dict(warp_density=5, block_size=32, batch_size=bsz, write_seed=1, spin_limit_ns=SPIN)
+        with g.Scheduler(eng, mode=g.SCHED_PLAIN) as plain:
+            rp = plain.run("tpl_nw", **kw)
+        with g.Scheduler(eng, mode=g.SCHED_LEARNED) as sc:
+            sc.run("tpl_nw", **kw)          # learns the network and the policy
+            rl = sc.run("tpl_nw", **kw)
+        assert rp["committed"] == rl["committed"] == len(txs)
+        gain = rl["tx_per_s"] / rp["tx_per_s"]
+        print(f"plain {rp['tx_per_s']:.0f} tx/s, learned {rl['tx_per_s']:.0f} tx/s, x{gain:.2f}; "
+              f"abort rate {rp['sched_abort_rate']:.3f} -> {rl['sched_abort_rate']:.3f}")
+        assert rl["sched_abort_rate"] < rp["sched_abort_rate"]
+        assert gain > 1.3
