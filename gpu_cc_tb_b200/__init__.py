@@ -118,6 +118,28 @@ class SchedResult(C.Structure):
                 ("predict_ms", C.c_double), ("train_ms", C.c_double), ("last_loss", C.c_double)]
 
 
+class OeDesc(C.Structure):
+    _fields_ = [("warehouses", C.c_uint32), ("districts", C.c_uint32), ("customers", C.c_uint32),
+                ("items", C.c_uint32), ("new_order_pct", C.c_uint32),
+                ("remote_line_permille", C.c_uint32), ("remote_customer_pct", C.c_uint32),
+                ("min_lines", C.c_uint32), ("max_lines", C.c_uint32)]
+
+
+class OeLayout(C.Structure):
+    _fields_ = [("warehouse", C.c_uint64), ("district", C.c_uint64), ("customer", C.c_uint64),
+                ("item", C.c_uint64), ("stock", C.c_uint64), ("inserts", C.c_uint64),
+                ("rows", C.c_uint64)]
+
+
+OP_ADD, OP_SUB, OP_STOCK, OP_PAY, OP_INSERT = 1, 2, 3, 4, 5
+F_EXT_OPS = 64
+
+
+def op_word(op: int, field: int, v: int) -> int:
+    """The `read` word of an extended request op (GCC_OP_WORD)."""
+    return int(np.int32(np.uint32(0x80000000 | (op << 28) | (field << 24) | (v & 0xFFFFFF)).view(np.int32)))
+
+
 SCHED_PLAIN, SCHED_LEARNED = 0, 1
 SCHED_FEAT_STRIDE = 72
 SCHED_SCHEMES = ["tpl_nw", "tpl_wd", "silo", "tictoc"]
@@ -169,6 +191,10 @@ def library() -> C.CDLL:
                                       C.POINTER(Result)]),
         "gcc_get_batch_stats": (C.c_int, [P, P, P, P, C.c_uint64]),
         "gcc_get_batch_active": (C.c_int, [P, P, C.c_uint64]),
+        "gcc_oe_offsets": (C.c_int, [C.POINTER(OeDesc), C.c_uint64, C.c_uint64, P,
+                                     C.POINTER(OeLayout)]),
+        "gcc_oe_gen": (C.c_int, [C.POINTER(OeDesc), C.c_uint64, C.c_uint64, C.c_int32, P, P, P]),
+        "gcc_oe_fill": (C.c_int, [P, C.POINTER(OeDesc), C.c_uint64]),
         "gcc_sched_param_count": (C.c_uint64, []),
         "gcc_sched_create": (C.c_int, [P, C.POINTER(SchedParams), C.POINTER(P)]),
         "gcc_sched_destroy": (None, [P]),
@@ -233,6 +259,26 @@ def gen_ycsb_var(rows: int, n_tx: int, theta: float, read_ratio: float, min_ops:
     _check(lib.gcc_gen_ycsb_var(rows, n_tx, theta, read_ratio, seed, key_base, threads,
                                 _ptr(off), _ptr(reqs)), "gcc_gen_ycsb_var")
     return off, reqs
+
+
+def order_entry_desc(warehouses: int = 64, districts: int = 10, customers: int = 3000,
+                     items: int = 100_000, new_order_pct: int = 50, remote_line_permille: int = 10,
+                     remote_customer_pct: int = 15, min_lines: int = 5, max_lines: int = 15) -> OeDesc:
+    return OeDesc(warehouses, districts, customers, items, new_order_pct, remote_line_permille,
+                  remote_customer_pct, min_lines, max_lines)
+
+
+def gen_order_entry(desc: OeDesc, n_tx: int, seed: int = 141919810, threads: int = 0):
+    """Order-entry transactions: (tx_off, reqs, kind, layout dict)."""
+    lib = library()
+    off = np.zeros(n_tx + 1, dtype=np.uint32)
+    lay = OeLayout()
+    _check(lib.gcc_oe_offsets(C.byref(desc), n_tx, seed, _ptr(off), C.byref(lay)), "gcc_oe_offsets")
+    reqs = np.zeros(int(off[-1]), dtype=REQ_DTYPE)
+    kind = np.zeros(n_tx, dtype=np.uint8)
+    _check(lib.gcc_oe_gen(C.byref(desc), n_tx, seed, threads, _ptr(off), _ptr(reqs), _ptr(kind)),
+           "gcc_oe_gen")
+    return off, reqs, kind, {k: getattr(lay, k) for k, _ in OeLayout._fields_}
 
 
 class Engine:
@@ -302,6 +348,10 @@ class Engine:
         self.last_result = r.as_dict()
         _check(rc, f"gcc_run_checked({scheme})")
         return r.as_dict(), v.value == 1
+
+    def oe_fill(self, desc: OeDesc, seed: int = 141919810):
+        """Initial order-entry rows (gcc_oe_fill)."""
+        _check(self.lib.gcc_oe_fill(self._h, C.byref(desc), seed), "gcc_oe_fill")
 
     def load_var_txs(self, tx_off: np.ndarray, reqs: np.ndarray):
         tx_off = np.ascontiguousarray(tx_off, dtype=np.uint32)

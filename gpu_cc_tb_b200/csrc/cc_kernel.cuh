@@ -94,6 +94,7 @@ struct TxOps {
     static constexpr int G = G_;
     static constexpr int MAXOPS = MO;
     static constexpr int K = (MO + G - 1) / G;
+    static constexpr bool kExt = MO > kMaxOps;  // extended ops (var-length only)
     uint32_t n;                // requests in the transaction
     uint32_t valid;            // bit k: op k exists
     uint32_t isread;           // bit k: op k reads
@@ -146,10 +147,66 @@ GCC_D int rowcopy_src(unsigned long long readmask, uint32_t i) {
     unsigned long long m = readmask & ((1ull << i) - 1ull);
     return m ? 63 - __clzll((long long)m) : -1;
 }
-// Apply write op i of tx to `row` (GCC_WRITE_FIELD or GCC_WRITE_ROWCOPY).
+// Extended write op (a request whose `read` word is negative, see
+// gcc_engine.h GCC_OP_*): an integer read-modify-write of row fields, or an
+// insert of a fresh row. Runs with the row held exclusively by the
+// transaction (2PL lock, OCC write lock at commit, TO uncommitted mark,
+// ordered turn); read-modify-writes fold the row image they read into the
+// digest like a read.
+GCC_D unsigned long long apply_ext(const KParams &p, uint64_t *r, uint32_t tx, uint32_t i,
+                                  uint32_t w) {
+    const uint32_t op = (w >> 28) & 7u, f = (w >> 24) & 15u, v = w & 0xFFFFFFu;
+    const uint32_t fmax = op == GCC_OP_STOCK ? 6u : (op == GCC_OP_PAY ? 7u : 9u);
+    if (op < GCC_OP_ADD || op > GCC_OP_INSERT || f > fmax || p.words != 11u) {
+        set_error(p.ctr, GCC_EFORMAT, 0);
+        return 0ull;
+    }
+    if (op == GCC_OP_INSERT) {
+        __stcg((unsigned long long *)(r + 1), (unsigned long long)tx);
+        __stcg((unsigned long long *)(r + 2), (unsigned long long)v);
+#pragma unroll
+        for (uint32_t k = 0; k < 8; ++k)
+            __stcg((unsigned long long *)(r + 3 + k),
+                   (unsigned long long)hash3(p.write_seed, tx, 1024ull + i * 8ull + k));
+        return 0ull;
+    }
+    unsigned long long dt = 0;
+    read_image(p, r, tx, 0, i, dt);
+    unsigned long long *fw = (unsigned long long *)(r + 1 + f);
+    const unsigned long long a = __ldcg(fw);
+    if (op == GCC_OP_ADD) {
+        __stcg(fw, a + v);
+    } else if (op == GCC_OP_SUB) {
+        __stcg(fw, a - v);
+    } else if (op == GCC_OP_STOCK) {
+        const unsigned long long q = v & 0xFFu, remote = (v >> 8) & 1u;
+        __stcg(fw, a >= q + 10u ? a - q : a - q + 91u);
+        __stcg(fw + 1, __ldcg(fw + 1) + q);
+        __stcg(fw + 2, __ldcg(fw + 2) + 1u);
+        __stcg(fw + 3, __ldcg(fw + 3) + remote);
+    } else if (op == GCC_OP_PAY) {
+        __stcg(fw, a - v);
+        __stcg(fw + 1, __ldcg(fw + 1) + v);
+        __stcg(fw + 2, __ldcg(fw + 2) + 1u);
+    }
+    return dt;
+}
+
+// Apply write op i of tx to `row` (GCC_WRITE_FIELD or GCC_WRITE_ROWCOPY, or
+// an extended op when the run enables them). Extended ops exist only in the
+// variable-length kernels (EXT): the 16-request kernels keep their registers.
+template <bool EXT>
 GCC_D void apply_write(const KParams &p, uint32_t row, uint32_t tx, uint64_t pos,
-                       uint32_t i, unsigned long long readmask) {
+                       uint32_t i, unsigned long long readmask, unsigned long long &dg) {
     uint64_t *r = row_ptr(p, row);
+    if (EXT && p.ext_ops) {
+        const int32_t w = p.txs ? __ldg(&p.txs[tx].requests[i].read)
+                                : __ldg(&p.reqs[p.tx_off[tx] + i].read);
+        if (w < 0) {
+            dg += apply_ext(p, r, tx, i, (uint32_t)w);
+            return;
+        }
+    }
     if (p.write_mode == GCC_WRITE_FIELD) {
         uint32_t f = write_field(p.write_seed, tx, i);
         __stcg((unsigned long long *)(r + 1 + f),
@@ -401,7 +458,7 @@ GCC_D int attempt_tpl(const KParams &p, const Group<G> &g, const TX &s, uint32_t
 #pragma unroll
     for (int k = 0; k < K; ++k)
         if (((s.valid & ~s.isread) >> k) & 1u)
-            apply_write(p, s.row[k], tx, pos, (uint32_t)(g.glane + k * G), s.readmask);
+            apply_write<TX::kExt>(p, s.row[k], tx, pos, (uint32_t)(g.glane + k * G), s.readmask, dg);
     // (the fast variants' unlocks are release operations)
     if (SLOW) fence_acq_rel();
     bool uerr = false;
@@ -568,7 +625,7 @@ GCC_D int attempt_to(const KParams &p, const Group<G> &g, const TX &s, uint32_t 
     if (p.write_mode == GCC_WRITE_ROWCOPY) g.sync();
 #pragma unroll
     for (int k = 0; k < K; ++k)
-        if ((wrote >> k) & 1u) apply_write(p, s.row[k], tx, pos, g.glane + k * G, s.readmask);
+        if ((wrote >> k) & 1u) apply_write<TX::kExt>(p, s.row[k], tx, pos, g.glane + k * G, s.readmask, dg);
     fence_acq_rel();
 #pragma unroll
     for (int k = 0; k < K; ++k)
@@ -704,7 +761,7 @@ GCC_D int attempt_mvcc(const KParams &p, const Group<G> &g, const TX &s, uint32_
         p.ver_prev[node] = ld_cg(p.turn + row);
         fence_acq_rel();
         atomicExch(p.turn + row, node);
-        apply_write(p, row, tx, pos, i, s.readmask);
+        apply_write<TX::kExt>(p, row, tx, pos, i, s.readmask, dg);
         fence_acq_rel();
         atomicExch(p.meta + row, tso::make(false, ts, ts));
     }
@@ -880,7 +937,7 @@ GCC_D int attempt_silo(const KParams &p, const Group<G> &g, const TX &s, uint32_
     if (p.write_mode == GCC_WRITE_ROWCOPY) g.sync();
 #pragma unroll
     for (int k = 0; k < K; ++k)
-        if ((writes >> k) & 1u) apply_write(p, s.row[k], tx, pos, g.glane + k * G, s.readmask);
+        if ((writes >> k) & 1u) apply_write<TX::kExt>(p, s.row[k], tx, pos, g.glane + k * G, s.readmask, dg);
     fence_acq_rel();
 #pragma unroll
     for (int k = 0; k < K; ++k)
@@ -1015,7 +1072,7 @@ GCC_D int attempt_tictoc(const KParams &p, const Group<G> &g, const TX &s, uint3
     if (p.write_mode == GCC_WRITE_ROWCOPY) g.sync();
 #pragma unroll
     for (int k = 0; k < K; ++k)
-        if ((writes >> k) & 1u) apply_write(p, s.row[k], tx, pos, g.glane + k * G, s.readmask);
+        if ((writes >> k) & 1u) apply_write<TX::kExt>(p, s.row[k], tx, pos, g.glane + k * G, s.readmask, dg);
     fence_acq_rel();
 #pragma unroll
     for (int k = 0; k < K; ++k)
@@ -1060,7 +1117,7 @@ GCC_D int attempt_ordered(const KParams &p, const Group<G> &g, const TX &s, uint
             if (rd) {
                 read_image(p, row_ptr(p, s.row[k]), tx, pos, i, dg);
             } else {
-                apply_write(p, s.row[k], tx, pos, i, s.readmask);
+                apply_write<TX::kExt>(p, s.row[k], tx, pos, i, s.readmask, dg);
             }
             // release: this access comes before the successor's
             st_release(p.turn + s.row[k], mypos[k] + 1u);
@@ -1205,7 +1262,7 @@ __global__ void __launch_bounds__(1024, 1) ycsb_kernel(const __grid_constant__ K
                 if constexpr (MO == kMaxOps) rq = __ldg((const int2 *)&T->requests[i]);
                 else rq = __ldg((const int2 *)(p.reqs + beg + i));
                 s.valid |= 1u << k;
-                if (rq.x) { s.isread |= 1u << k; myreads |= 1ull << i; }
+                if (rq.x > 0) { s.isread |= 1u << k; myreads |= 1ull << i; }
                 if constexpr (is_ordered(SCH)) {
                     s.row[k] = __ldg(p.op_row + pos * p.slot_ops + i);
                 } else {

@@ -527,6 +527,17 @@ int gcc_load_txs(gcc_engine *e, const gcc_ycsb_tx *txs, uint64_t n_tx) {
     return GCC_OK;
 }
 
+}  // extern "C"
+
+// Runs with GCC_F_EXT_OPS: not under MVCC (versions hold whole rows written
+// blindly), only on the u64 field layout with field writes.
+static bool ext_ops_allowed(const gcc_engine *e, int s, const gcc_run_params *rp) {
+    if (!(rp->flags & GCC_F_EXT_OPS)) return true;
+    return !is_mvcc(s) && e->desc.layout == GCC_LAYOUT_U64X11 && rp->write_mode == GCC_WRITE_FIELD;
+}
+
+extern "C" {
+
 int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
     cudaGetLastError();  // a stale error of an earlier call is not ours
     if (!e || !rp || !out) return GCC_EINVAL;
@@ -539,6 +550,7 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
     if (rp->block_size < 1 || rp->block_size > 32) return GCC_EINVAL;
     if (rp->batch_size < 1) return GCC_EINVAL;
     if (rp->write_mode != GCC_WRITE_FIELD && rp->write_mode != GCC_WRITE_ROWCOPY) return GCC_EINVAL;
+    if (rp->flags & GCC_F_EXT_OPS) return GCC_EINVAL;  // variable-length runs only
     if (!e->txs || e->n_rec == 0) return GCC_ESTATE;
     cudaSetDevice(e->dev);
     e->n_tx = e->n_rec;  // outputs of this run cover the records
@@ -819,6 +831,7 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
     if (rp->warp_density < 2 || rp->warp_density > 5) return GCC_EINVAL;
     if (rp->block_size < 1 || rp->block_size > 32) return GCC_EINVAL;
     if (rp->write_mode != GCC_WRITE_FIELD) return GCC_EINVAL;
+    if (!ext_ops_allowed(e, s, rp)) return GCC_EINVAL;
     if (rp->backoff_ns < -1 || rp->backoff_ns > 100000) return GCC_EINVAL;
     if (!e->n_var || !e->reqs_d) return GCC_ESTATE;
     if (batch_off[0] != 0 || batch_off[nb] != e->n_var) return GCC_EINVAL;
@@ -897,6 +910,7 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
     p.spin_limit_ns = rp->spin_limit_ns ? rp->spin_limit_ns : 4000000000ull;
     p.backoff_ns = rp->backoff_ns < 0 ? 0u : (rp->backoff_ns == 0 ? 512u : (uint32_t)rp->backoff_ns);
     p.starve_limit = starve_param(rp->starve_limit);
+    p.ext_ops = (rp->flags & GCC_F_EXT_OPS) ? 1u : 0u;
     p.ver_ts = e->ver_ts;
     p.ver_prev = e->ver_prev;
     p.ver_data = e->ver_data;
@@ -1216,6 +1230,57 @@ int gcc_dump_table(gcc_engine *e, void *dst, uint64_t bytes) {
     cudaSetDevice(e->dev);
     cudaError_t ce = cudaMemcpy2DAsync(dst, e->row_bytes, e->table, e->stride, e->row_bytes,
                                        e->rows, cudaMemcpyDeviceToHost, e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    return ce == cudaSuccess ? GCC_OK : e->fail_cuda(ce);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Initial order-entry rows (see gcc_oe_fill): one thread per row.
+__global__ void k_oe_fill(uint8_t *table, uint64_t rows, uint32_t stride, gcc_oe_layout L,
+                          uint64_t seed) {
+    const uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    unsigned long long f[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    auto h = [&](uint32_t k) { return hash3(seed, r, k); };
+    if (r < L.district) {
+        f[0] = 30000000ull; f[1] = h(1) % 2001ull;
+    } else if (r < L.customer) {
+        f[0] = 3000000ull; f[1] = h(1) % 2001ull; f[2] = 3001ull;
+    } else if (r < L.item) {
+        f[0] = (unsigned long long)(-1000ll); f[1] = 1000ull; f[2] = 1ull; f[3] = h(3) % 5001ull;
+    } else if (r < L.stock) {
+        f[0] = 100ull + h(0) % 9901ull;
+    } else if (r < L.inserts) {
+        f[0] = 10ull + h(0) % 91ull;
+    }
+    unsigned long long *w = (unsigned long long *)(table + r * stride);
+    w[0] = r;
+#pragma unroll
+    for (int k = 0; k < 10; ++k) w[1 + k] = f[k];
+    for (uint32_t k = 11; k < stride / 8; ++k) w[k] = 0ull;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gcc_oe_fill(gcc_engine *e, const gcc_oe_desc *d, uint64_t seed) {
+    cudaGetLastError();
+    if (!e || !d) return GCC_EINVAL;
+    if (e->desc.layout != GCC_LAYOUT_U64X11) return GCC_EINVAL;
+    gcc_oe_layout L;
+    std::vector<uint32_t> off(2);
+    int rc = gcc_oe_offsets(d, 0, seed, off.data(), &L);
+    if (rc) return rc;
+    if (e->rows < L.rows) return GCC_EINVAL;
+    cudaSetDevice(e->dev);
+    k_oe_fill<<<(unsigned)((e->rows + 255) / 256), 256, 0, e->stream>>>(e->table, e->rows, e->stride,
+                                                                      L, seed);
+    e->kernel_launches += 1;
+    cudaError_t ce = cudaGetLastError();
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
     return ce == cudaSuccess ? GCC_OK : e->fail_cuda(ce);
 }
@@ -1566,7 +1631,7 @@ int gcc_sched_run(gcc_sched *sc, const gcc_run_params *rp, gcc_sched_result *out
     if (rp->block_size < 1 || rp->block_size > 32) return GCC_EINVAL;
     if (rp->batch_size < 1 || rp->batch_size > (1 << 20)) return GCC_EINVAL;
     if (rp->write_mode != GCC_WRITE_FIELD) return GCC_EINVAL;
-    if (rp->flags & (GCC_F_READ_LOG | GCC_F_AUTOTUNE | GCC_F_GRAPH)) return GCC_EINVAL;
+    if (rp->flags & (GCC_F_READ_LOG | GCC_F_AUTOTUNE | GCC_F_GRAPH | GCC_F_EXT_OPS)) return GCC_EINVAL;
     if (rp->backoff_ns < -1 || rp->backoff_ns > 100000) return GCC_EINVAL;
     if (rp->max_active < 0 || rp->starve_limit < -1) return GCC_EINVAL;
     if (!e->txs || e->n_rec == 0) return GCC_ESTATE;

@@ -174,6 +174,7 @@ struct KParams {
     uint32_t wait_die;
     uint32_t backoff_ns;        // 0: retry at once
     uint32_t starve_limit;      // 0: no starvation control
+    uint32_t ext_ops;           // the loaded transactions hold extended ops
 };
 
 // ---------------------------------------------------------------------------

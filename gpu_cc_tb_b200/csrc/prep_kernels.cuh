@@ -242,7 +242,7 @@ __global__ void k_access_build(KParams p, uint64_t n_pos, uint32_t invalid_key, 
         row = index_find(p, (uint32_t)rq.y);
         if (row == kNoRow) atomicCAS(&p.ctr->err, 0u, (unsigned)GCC_EKEY);
         else key = row;
-        rd = rq.x ? 1u : 0u;
+        rd = rq.x > 0 ? 1u : 0u;
     }
     keys[a] = key;
     vals[a] = (uint32_t)a | (rd << 31);

@@ -35,7 +35,7 @@ __global__ void k_features(const gcc_ycsb_tx *__restrict__ txs, uint64_t first, 
             const int2 rq = *(const int2 *)&T->requests[l];
             const uint32_t key = (uint32_t)rq.y;
             bin = sketch_bin(key);
-            wr = rq.x ? 0u : 1u;
+            wr = rq.x > 0 ? 0u : 1u;
             hot = heat(__ldg(freq + freq_slot(key)));
         }
     }

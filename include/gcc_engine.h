@@ -75,6 +75,34 @@ extern "C" {
 #define GCC_F_RETRY_IMMEDIATE 8u /* retry an aborted transaction at once
                                instead of first waiting (up to 50 us) until
                                the row that made it abort looks free */
+#define GCC_F_EXT_OPS 64u   /* requests with a negative `read` word are
+                               extended ops (GCC_OP_*); without this flag
+                               every request with read <= 0 is a YCSB write */
+
+/* ---- extended request ops ------------------------------------------------
+ * A request whose `read` word is negative is an integer write op on the u64
+ * key + 10 field layout (no counterpart in the reference's YCSB records,
+ * whose `read` is 0 or 1): bits 28-30 opcode, 24-27 field f (0-9), 0-23
+ * parameter v; write with GCC_OP_WORD. Read-modify-write ops return the row
+ * they read in the transaction's digest, like a read; an insert does not.
+ *   ADD    field f += v
+ *   SUB    field f -= v (two's complement)
+ *   STOCK  q = v & 0xFF, remote = v >> 8 & 1: field f = f >= q + 10 ? f - q
+ *          : f - q + 91; f+1 += q; f+2 += 1; f+3 += remote   (f <= 6)
+ *   PAY    field f -= v; f+1 += v; f+2 += 1                   (f <= 7)
+ *   INSERT field 0 = transaction id, field 1 = v, fields 2-9 = a hash of
+ *          (write_seed, transaction id, op index)
+ * Enabled per run by GCC_F_EXT_OPS on variable-length transactions
+ * (gcc_load_var_txs + gcc_run_batches / gcc_serve). Schemes: tpl_nw, tpl_wd,
+ * to, silo, tictoc; layout GCC_LAYOUT_U64X11, write mode GCC_WRITE_FIELD. A
+ * malformed op word ends the run with GCC_EFORMAT. */
+#define GCC_OP_ADD 1
+#define GCC_OP_SUB 2
+#define GCC_OP_STOCK 3
+#define GCC_OP_PAY 4
+#define GCC_OP_INSERT 5
+#define GCC_OP_WORD(op, field, v) \
+    ((int32_t)(0x80000000u | ((uint32_t)(op) << 28) | ((uint32_t)(field) << 24) | ((uint32_t)(v) & 0xFFFFFFu)))
 
 /* Dataset generator dedup modes (gen_ycsb drops repeated keys, which leaves
  * fewer than 16 requests; resample redraws until 16 distinct keys). */
@@ -185,6 +213,56 @@ int gcc_gen_ycsb_var_offsets(uint64_t n_tx, uint32_t min_ops, uint32_t max_ops,
 int gcc_gen_ycsb_var(uint64_t rows, uint64_t n_tx, double theta, double read_ratio,
                      uint64_t seed, int32_t key_base, int32_t threads,
                      const uint32_t *tx_off, gcc_ycsb_req *reqs);
+
+/* ---- Order-entry workload (integer; shape of the reference's TPC-C
+ * new-order / payment path, benchmark/tpcc.cu:35-380 and
+ * generation/gen_tpcc.cu:108-182, with money in integer cents instead of
+ * floats and inserted rows at ids assigned at generation). Transactions are
+ * variable-length requests with extended ops (GCC_OP_*), sorted by row id;
+ * run them with GCC_F_EXT_OPS on an engine of `rows` rows with the direct
+ * index, after gcc_oe_fill. Row groups and fields:
+ *   warehouse w                 0 ytd cents, 1 tax bp
+ *   district  w*D + d           0 ytd, 1 tax, 2 next_o_id
+ *   customer  (w*D + d)*C + c   0 balance (signed), 1 ytd_payment,
+ *                               2 payment_cnt, 3 discount bp
+ *   item      i                 0 price cents (read only)
+ *   stock     w*I + i           0 quantity, 1 ytd, 2 order_cnt, 3 remote_cnt
+ *   inserts                     one slot per inserted row
+ * new-order: read warehouse, district next_o_id += 1, read customer, per
+ * line read item + STOCK update + insert order line, insert order (4 + 3 x
+ * lines requests); payment: warehouse and district ytd += amount, customer
+ * PAY, insert history (4 requests). */
+typedef struct gcc_oe_desc {
+    uint32_t warehouses;           /* W (64 in the serving workload) */
+    uint32_t districts;            /* D per warehouse (10) */
+    uint32_t customers;            /* C per district (3000) */
+    uint32_t items;                /* I, also stock rows per warehouse (100000) */
+    uint32_t new_order_pct;        /* share of new-order transactions (50) */
+    uint32_t remote_line_permille; /* order lines from another warehouse (10) */
+    uint32_t remote_customer_pct;  /* payments of another warehouse's customer (15) */
+    uint32_t min_lines, max_lines; /* order lines per new-order (5, 15) */
+} gcc_oe_desc;
+
+typedef struct gcc_oe_layout {
+    uint64_t warehouse, district, customer, item, stock, inserts; /* first rows */
+    uint64_t rows;                                                /* total rows */
+} gcc_oe_layout;
+
+/* Request offsets of n_tx transactions (tx_off[n_tx + 1]) and the row
+ * layout they need; pure functions of (desc, seed, transaction index). */
+int gcc_oe_offsets(const gcc_oe_desc *d, uint64_t n_tx, uint64_t seed, uint32_t *tx_off,
+                   gcc_oe_layout *layout);
+/* The requests (reqs[tx_off[n_tx]]); kind[t] = 1 new-order, 2 payment
+ * (optional). `threads` host threads (0 = all). */
+int gcc_oe_gen(const gcc_oe_desc *d, uint64_t n_tx, uint64_t seed, int32_t threads,
+               const uint32_t *tx_off, gcc_ycsb_req *reqs, uint8_t *kind);
+/* Initial order-entry rows on the device (the engine's rows must be at least
+ * layout.rows of the same desc; inserts area and unused fields zero):
+ * warehouse ytd 30,000,000 and tax h % 2001; district ytd 3,000,000, tax
+ * h % 2001, next_o_id 3001; customer balance -1000, ytd_payment 1000,
+ * payment_cnt 1, discount h % 5001; item price 100 + h % 9901; stock
+ * quantity 10 + h % 91; h = splitmix-based hash of (seed, row, field). */
+int gcc_oe_fill(gcc_engine *e, const gcc_oe_desc *d, uint64_t seed);
 
 /* Engine lifetime (Table_CPU::InitData + AddIndex + DB_CPU::ToGPU). */
 int gcc_create(const gcc_table_desc *desc, gcc_engine **out);

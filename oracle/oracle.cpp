@@ -38,6 +38,47 @@ uint64_t load_word(const uint8_t *p) {
 }
 void store_word(uint8_t *p, uint64_t v) { memcpy(p, &v, 8); }
 
+// Extended write op (request `read` < 0, gcc_engine.h GCC_OP_*) on a packed
+// u64 row of `words` words: returns the digest term of the row image it
+// reads (read-modify-writes) or 0 (insert); GCC_EFORMAT via *bad.
+uint64_t ext_op(uint8_t *r, uint32_t words, uint32_t w, uint64_t wseed, uint32_t tx, uint32_t i,
+                bool *bad) {
+    const uint32_t op = (w >> 28) & 7u, f = (w >> 24) & 15u, v = w & 0xFFFFFFu;
+    const uint32_t fmax = op == GCC_OP_STOCK ? 6u : (op == GCC_OP_PAY ? 7u : 9u);
+    if (op < GCC_OP_ADD || op > GCC_OP_INSERT || f > fmax || words != 11u) {
+        *bad = true;
+        return 0;
+    }
+    auto fld = [&](uint32_t k) { return r + 8 * (1 + k); };
+    if (op == GCC_OP_INSERT) {
+        store_word(fld(0), tx);
+        store_word(fld(1), v);
+        for (uint32_t k = 0; k < 8; ++k) store_word(fld(2 + k), h3(wseed, tx, 1024ull + i * 8ull + k));
+        return 0;
+    }
+    uint64_t dt = 0;
+    for (uint32_t k = 0; k < words; ++k) dt += term(load_word(r + 8 * k), i, k);
+    const uint64_t a = load_word(fld(f));
+    switch (op) {
+        case GCC_OP_ADD: store_word(fld(f), a + v); break;
+        case GCC_OP_SUB: store_word(fld(f), a - v); break;
+        case GCC_OP_STOCK: {
+            const uint64_t q = v & 0xFFu, remote = (v >> 8) & 1u;
+            store_word(fld(f), a >= q + 10 ? a - q : a - q + 91);
+            store_word(fld(f + 1), load_word(fld(f + 1)) + q);
+            store_word(fld(f + 2), load_word(fld(f + 2)) + 1);
+            store_word(fld(f + 3), load_word(fld(f + 3)) + remote);
+            break;
+        }
+        case GCC_OP_PAY:
+            store_word(fld(f), a - v);
+            store_word(fld(f + 1), load_word(fld(f + 1)) + v);
+            store_word(fld(f + 2), load_word(fld(f + 2)) + 1);
+            break;
+    }
+    return dt;
+}
+
 struct Ctx {
     uint8_t *table;
     uint64_t rows;
@@ -60,7 +101,7 @@ int run_serial(const Ctx &c, const gcc_ycsb_tx &tx, uint32_t txid, uint64_t *dig
         uint64_t row = rq.key;  // keys are row ids (row r holds key r)
         if (row >= c.rows) return GCC_EKEY;
         uint8_t *r = c.table + row * c.rb;
-        if (rq.read) {
+        if (rq.read > 0) {
             for (uint32_t k = 0; k < c.words; ++k) dg += term(load_word(r + 8 * k), i, k);
             memcpy(item.data(), r, c.rb);
             if (read_log) memcpy(read_log + ((uint64_t)txid * 16 + i) * rstride(c.layout), r, c.rb);
@@ -95,6 +136,14 @@ int oracle_replay_var(uint8_t *table, uint64_t rows, int32_t layout, const uint3
                       const gcc_ycsb_req *reqs, uint64_t n_tx, const uint32_t *order,
                       uint64_t n_order, int32_t write_mode, uint64_t write_seed,
                       uint64_t *digests) {
+    return oracle_replay_var_ext(table, rows, layout, tx_off, reqs, n_tx, order, n_order,
+                                 write_mode, write_seed, digests, 0);
+}
+
+int oracle_replay_var_ext(uint8_t *table, uint64_t rows, int32_t layout, const uint32_t *tx_off,
+                          const gcc_ycsb_req *reqs, uint64_t n_tx, const uint32_t *order,
+                          uint64_t n_order, int32_t write_mode, uint64_t write_seed,
+                          uint64_t *digests, int32_t ext_ops) {
     Ctx c{table, rows, layout, rbytes(layout), rbytes(layout) / 8, write_mode, write_seed};
     std::vector<uint8_t> item(c.rb);
     for (uint64_t j = 0; j < n_order; ++j) {
@@ -108,9 +157,13 @@ int oracle_replay_var(uint8_t *table, uint64_t rows, int32_t layout, const uint3
             const gcc_ycsb_req &rq = reqs[tx_off[t] + i];
             if (rq.key >= rows) return GCC_EKEY;
             uint8_t *r = c.table + (uint64_t)rq.key * c.rb;
-            if (rq.read) {
+            if (rq.read > 0) {
                 for (uint32_t k = 0; k < c.words; ++k) dg += term(load_word(r + 8 * k), i, k);
                 memcpy(item.data(), r, c.rb);
+            } else if (ext_ops && rq.read < 0) {
+                bool bad = false;
+                dg += ext_op(r, c.words, (uint32_t)rq.read, c.wseed, t, i, &bad);
+                if (bad) return GCC_EFORMAT;
             } else if (c.write_mode == GCC_WRITE_FIELD) {
                 uint32_t f = (uint32_t)(h3(c.wseed, t, 2ull * i) % 10ull);
                 store_word(r + 8 * (1 + f), h3(c.wseed, t, 2ull * i + 1));

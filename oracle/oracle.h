@@ -51,6 +51,15 @@ int oracle_replay_var(uint8_t *table, uint64_t rows, int32_t layout, const uint3
                       uint64_t n_order, int32_t write_mode, uint64_t write_seed,
                       uint64_t *digests);
 
+/* The same with extended ops (gcc_engine.h GCC_OP_*) when ext_ops != 0:
+ * requests with a negative `read` word apply their integer read-modify-write
+ * or insert, read-modify-writes adding the row image they read to the
+ * digest. */
+int oracle_replay_var_ext(uint8_t *table, uint64_t rows, int32_t layout, const uint32_t *tx_off,
+                          const gcc_ycsb_req *reqs, uint64_t n_tx, const uint32_t *order,
+                          uint64_t n_order, int32_t write_mode, uint64_t write_seed,
+                          uint64_t *digests, int32_t ext_ops);
+
 /* GPUTx execution order: ranks per tx (reference rank function), and the
  * txs sorted by (rank, tx). */
 int oracle_gputx_order(const gcc_ycsb_tx *txs, uint64_t n_tx, uint64_t rows, uint32_t *ranks,

@@ -35,6 +35,7 @@ def lib():
             "oracle_replay": [P, U64, I32, P, U64, P, U64, I32, U64, P, P],
             "oracle_gputx_order": [P, U64, U64, P, P, P],
             "oracle_replay_var": [P, U64, I32, P, P, U64, P, U64, I32, U64, P],
+            "oracle_replay_var_ext": [P, U64, I32, P, P, U64, P, U64, I32, U64, P, I32],
             "oracle_commit_order": [P, U64, P],
             "oracle_conflict_acyclic": [P, U64, U64],
             "oracle_cpu_run": [C.c_char_p, P, U64, I32, P, U64, I32, U64, I32, P, P,
@@ -84,16 +85,17 @@ def replay(table, layout, txs, order, write_mode, write_seed, read_log=False):
     return t, dg, rl
 
 
-def replay_var(table, layout, tx_off, reqs, order, write_mode, write_seed):
-    """Serial replay of variable-length transactions (CSR)."""
+def replay_var(table, layout, tx_off, reqs, order, write_mode, write_seed, ext_ops=False):
+    """Serial replay of variable-length transactions (CSR); ext_ops applies
+    extended request ops (negative `read` words)."""
     t = np.array(table, dtype=np.uint8, copy=True)
     n = len(tx_off) - 1
     dg = np.zeros(n, dtype=np.uint64)
     order = np.ascontiguousarray(np.arange(n) if order is None else order, dtype=np.uint32)
     tx_off = np.ascontiguousarray(tx_off, dtype=np.uint32)
     reqs = np.ascontiguousarray(reqs)
-    rc = lib().oracle_replay_var(_p(t), t.shape[0], layout, _p(tx_off), _p(reqs), n, _p(order),
-                                 len(order), write_mode, write_seed, _p(dg))
+    rc = lib().oracle_replay_var_ext(_p(t), t.shape[0], layout, _p(tx_off), _p(reqs), n, _p(order),
+                                     len(order), write_mode, write_seed, _p(dg), 1 if ext_ops else 0)
     if rc != 0:
         raise RuntimeError(f"oracle_replay_var failed: {rc}")
     return t, dg
