@@ -12,6 +12,7 @@ kernels, gCCTB's tot_time definition, benchmark_cpu/ycsb.cu:249-291).
   python bench.py --impl reference ...   # the CPU executor on the host cores
   python bench.py --workload batched ...  # 64 uneven batches, 4-64 requests/tx
   python bench.py --workload learned ...  # drifting contention, learned scheduling
+  python bench.py --workload serving ...  # order-entry arrivals, p50/p99 latency
 
 The batched workload: 64 consecutive batches with log-uniform sizes in
 [4096, 262144] transactions of 4-64 requests (uniform), theta 0.8, read ratio
@@ -24,6 +25,14 @@ requests on the same table, Zipf theta drifting linearly from 0.5 to 0.99
 and read ratio from 0.9 to 0.5 across the batches; the learned scheduler
 (BF16 MLP contention predictor, deferral into capped sub-batches, measured
 policy) against plain ordering on identical batches through the same driver.
+
+The serving workload: integer order-entry transactions (64 warehouses x 10
+districts x 3,000 customers, 100,000 items and stock rows per warehouse;
+50% new-order with 5-15 NURand(8191) lines, 1% remote lines; 50% payment,
+15% remote customers, 1-5000 cents) arriving as a Poisson process at 10% to
+120% of the measured peak rate; batches admitted by free device memory,
+table and CC state resident; p50/p99 arrival-to-commit latency and commits/s
+with the learned scheduler on and off.
 
 Multi-GPU runs are independent replicas (the path does not shard): every
 rank runs the whole workload on its own GPU; value = all ranks' committed
@@ -68,7 +77,8 @@ def parse():
     ap.add_argument("--cpu-threads", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweep", default="", help="comma list of extra schemes to time once")
-    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "learned"],
+    ap.add_argument("--workload", default="plain",
+                    choices=["plain", "batched", "learned", "serving"],
                     help="plain: 1,048,576 x 16-request transactions in 65,536 batches; "
                          "batched: 64 uneven batches of 4-64-request transactions; "
                          "learned: 256 drifting-contention batches, learned scheduling")
@@ -478,6 +488,101 @@ def run_learned(a):
         dist.destroy_process_group()
 
 
+def run_serving(a):
+    """Order-entry serving: peak (saturated) commits/s and a Poisson load
+    sweep with p50/p99 latency, learned scheduler on vs off."""
+    from gpu_cc_tb_b200 import replicas
+    rank, ws, local, dist = replicas.init_from_env("nccl")
+    import torch  # noqa: F401  (CUDA context for the replicas' barrier)
+    import gpu_cc_tb_b200 as g
+    sch = a.scheme if a.scheme in g.SCHED_SCHEMES else "tpl_nw"
+    d = g.order_entry_desc()
+    n_all = 1_500_000
+    off, reqs, kind, lay = g.gen_order_entry(d, n_all, seed=141919810)
+    eng = g.Engine(lay["rows"], layout=g.LAYOUT_U64X11, index=g.INDEX_DIRECT, fill_seed=0,
+                   device=local, max_batch=65536)
+    eng.oe_fill(d, seed=141919810)
+    kw = dict(warp_density=a.wd, block_size=a.bs, flags=g.F_EXT_OPS | g.F_NO_RESET, write_seed=1)
+
+    def load(n):
+        eng.load_var_txs(off[:n + 1], reqs[:int(off[n])])
+
+    on = g.Scheduler(eng, mode=g.SCHED_LEARNED, seed=7)
+    off_s = g.Scheduler(eng, mode=g.SCHED_PLAIN)
+    n_peak = 600_000
+    load(n_peak)
+    for _ in range(max(1, a.warmup)):
+        on.serve(sch, rate_tps=1e10, seed=1, max_batch=65536, **kw)   # trains, settles
+        off_s.serve(sch, rate_tps=1e10, seed=1, max_batch=65536, **kw)
+    clocks = Clocks(local)
+    replicas.barrier(dist)
+    clocks.start()
+    peak = {"on": [], "off": []}
+    dev = {"on": [], "off": []}
+    for _ in range(a.steps):
+        r = on.serve(sch, rate_tps=1e10, seed=2, max_batch=65536, **kw)
+        peak["on"].append(r["tx_per_s"])
+        dev["on"].append(r["device_tx_per_s"])
+        r = off_s.serve(sch, rate_tps=1e10, seed=2, max_batch=65536, **kw)
+        peak["off"].append(r["tx_per_s"])
+        dev["off"].append(r["device_tx_per_s"])
+    replicas.barrier(dist)
+    clk = clocks.stop()
+    p_on, p_off = statistics.median(peak["on"]), statistics.median(peak["off"])
+    # end to end: upload of the request stream + saturated serving
+    e2e_s = 0.0
+    for _ in range(a.steps):
+        s0 = time.perf_counter()
+        load(n_peak)
+        on.serve(sch, rate_tps=1e10, seed=3, max_batch=65536, **kw)
+        e2e_s += time.perf_counter() - s0
+    # Poisson load sweep relative to the plain peak
+    sweep = []
+    for frac in (0.1, 0.25, 0.5, 0.75, 0.9, 1.0, 1.2):
+        rate = frac * p_off
+        n = int(min(n_all, max(20_000, rate * 1.5)))
+        load(n)
+        pt = {"load": frac, "rate_tps": rate, "transactions": n}
+        for name, sc in (("on", on), ("off", off_s)):
+            r = sc.serve(sch, rate_tps=rate, seed=11, max_batch=65536, **kw)
+            pt[name] = {"tx_per_s": r["tx_per_s"], "p50_us": r["lat_p50_us"],
+                        "p99_us": r["lat_p99_us"], "mean_batch": r["mean_batch"],
+                        "abort_rate": r["sched_abort_rate"]}
+        sweep.append(pt)
+    job = replicas.combine(dist, n_peak * a.steps / p_on, n_peak * a.steps, e2e_s, a.steps * n_peak)
+    if rank == 0:
+        line = {
+            "metric": "committed tx/s (learned vs plain CC, same GPU, 0 violations); p99",
+            "value": job["value"], "unit": "tx/s", "n_gpus": ws, "steps": a.steps,
+            "warmup": max(1, a.warmup), "ms_per_step": 1000 * n_peak / p_on,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded order-entry generator, Poisson arrivals)",
+            "config": {"workload": "order_entry_serving_W64_D10_C3000_I100000_50no_50pay",
+                       "cc_scheme": sch, "rows": lay["rows"], "warp_density": a.wd,
+                       "block_size": a.bs, "peak_transactions": n_peak,
+                       "admission": "all arrived, at most 65,536 per batch",
+                       "state": "table and CC metadata resident (no per-batch reset)",
+                       "parallelism": f"replicas x{ws}"},
+            "peak": {"learned_tx_per_s": p_on, "plain_tx_per_s": p_off,
+                     "speedup": p_on / p_off,
+                     "learned_device_tx_per_s": statistics.median(dev["on"]),
+                     "plain_device_tx_per_s": statistics.median(dev["off"])},
+            "sweep": sweep,
+            "e2e": {"value": job["e2e_value"], "unit": "tx/s",
+                    "h2d_bytes_per_step": int(reqs[:int(off[n_peak])].nbytes + 4 * (n_peak + 1)),
+                    "d2h_bytes_per_step": 0},
+            "gpu_launches": None,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    on.close()
+    off_s.close()
+    eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -488,6 +593,9 @@ def main():
         return
     if a.workload == "learned":
         run_learned(a)
+        return
+    if a.workload == "serving":
+        run_serving(a)
         return
     from gpu_cc_tb_b200 import replicas
     rank, ws, local, dist = replicas.init_from_env("nccl")

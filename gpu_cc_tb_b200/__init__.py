@@ -100,7 +100,8 @@ _LIB = None
 class SchedParams(C.Structure):
     _fields_ = [("mode", C.c_int32), ("explore_every", C.c_int32), ("probe_rows", C.c_int32),
                 ("train_steps", C.c_int32), ("minibatch", C.c_int32), ("lr", C.c_float),
-                ("defer_threshold", C.c_float), ("fixed_arm", C.c_int32), ("seed", C.c_uint64)]
+                ("defer_threshold", C.c_float), ("fixed_arm", C.c_int32), ("min_sched", C.c_int32),
+                ("reserved", C.c_int32), ("seed", C.c_uint64)]
 
 
 class SchedBatch(C.Structure):
@@ -138,6 +139,19 @@ F_EXT_OPS = 64
 def op_word(op: int, field: int, v: int) -> int:
     """The `read` word of an extended request op (GCC_OP_WORD)."""
     return int(np.int32(np.uint32(0x80000000 | (op << 28) | (field << 24) | (v & 0xFFFFFF)).view(np.int32)))
+
+
+class ServeParams(C.Structure):
+    _fields_ = [("rate_tps", C.c_double), ("seed", C.c_uint64), ("max_batch", C.c_int32),
+                ("min_batch", C.c_int32), ("max_wait_us", C.c_double)]
+
+
+class ServeResult(C.Structure):
+    _fields_ = [("committed", C.c_uint64), ("aborts", C.c_uint64), ("batches", C.c_uint64),
+                ("admit_cap", C.c_uint64), ("offered_tps", C.c_double), ("tx_per_s", C.c_double),
+                ("device_tx_per_s", C.c_double), ("lat_p50_us", C.c_double),
+                ("lat_p99_us", C.c_double), ("lat_max_us", C.c_double), ("mean_batch", C.c_double),
+                ("busy_frac", C.c_double), ("sched_abort_rate", C.c_double)]
 
 
 SCHED_PLAIN, SCHED_LEARNED = 0, 1
@@ -196,12 +210,16 @@ def library() -> C.CDLL:
         "gcc_oe_gen": (C.c_int, [C.POINTER(OeDesc), C.c_uint64, C.c_uint64, C.c_int32, P, P, P]),
         "gcc_oe_fill": (C.c_int, [P, C.POINTER(OeDesc), C.c_uint64]),
         "gcc_sched_param_count": (C.c_uint64, []),
+        "gcc_serve": (C.c_int, [P, C.POINTER(RunParams), C.POINTER(ServeParams),
+                                C.POINTER(ServeResult)]),
         "gcc_sched_create": (C.c_int, [P, C.POINTER(SchedParams), C.POINTER(P)]),
         "gcc_sched_destroy": (None, [P]),
         "gcc_sched_run": (C.c_int, [P, C.POINTER(RunParams), C.POINTER(SchedResult)]),
         "gcc_sched_batches": (C.c_int, [P, P, C.c_uint64]),
         "gcc_sched_features": (C.c_int, [P, C.c_uint64, C.c_uint64, P]),
         "gcc_sched_observe": (C.c_int, [P, C.c_uint64, C.c_uint64, C.c_int32]),
+        "gcc_sched_features_var": (C.c_int, [P, C.c_uint64, C.c_uint64, P]),
+        "gcc_sched_observe_var": (C.c_int, [P, C.c_uint64, C.c_uint64, C.c_int32]),
         "gcc_sched_set_weights": (C.c_int, [P, P, C.c_uint64]),
         "gcc_sched_get_weights": (C.c_int, [P, P, C.c_uint64]),
         "gcc_sched_predict": (C.c_int, [P, P, C.c_uint64, P]),
@@ -439,12 +457,13 @@ class Scheduler:
 
     def __init__(self, engine: "Engine", mode: int = SCHED_LEARNED, explore_every: int = 0,
                  probe_rows: int = 0, train_steps: int = 0, minibatch: int = 0, lr: float = 0.0,
-                 defer_threshold: float = 0.0, fixed_arm: int = 0, seed: int = 1):
+                 defer_threshold: float = 0.0, fixed_arm: int = 0, min_sched: int = 0,
+                 seed: int = 1):
         self.engine = engine
         self.lib = engine.lib
         self._h = C.c_void_p()
         prm = SchedParams(mode, explore_every, probe_rows, train_steps, minibatch, lr,
-                          defer_threshold, fixed_arm, seed)
+                          defer_threshold, fixed_arm, min_sched, 0, seed)
         _check(self.lib.gcc_sched_create(engine._h, C.byref(prm), C.byref(self._h)),
                "gcc_sched_create")
         self.n_params = int(self.lib.gcc_sched_param_count())
@@ -474,6 +493,21 @@ class Scheduler:
         _check(rc, f"gcc_sched_run({scheme}) err_site={r.run.err_site}")
         return out
 
+    def serve(self, scheme: str, rate_tps: float, seed: int = 1, max_batch: int = 0,
+              min_batch: int = 0, max_wait_us: float = 0.0, **kw) -> dict:
+        """Serve the engine's loaded variable-length transactions as a Poisson
+        arrival stream (gcc_serve); latencies are arrival -> commit."""
+        p = self.engine.params(scheme, **kw)
+        sp = ServeParams(rate_tps, seed, max_batch, min_batch, max_wait_us)
+        r = ServeResult()
+        rc = self.lib.gcc_serve(self._h, C.byref(p), C.byref(sp), C.byref(r))
+        out = {k: getattr(r, k) for k, _ in ServeResult._fields_}
+        self.last_result = out
+        self._nb = int(r.batches)
+        self.engine.n_tx = self.engine.n_var
+        _check(rc, f"gcc_serve({scheme})")
+        return out
+
     def batches(self) -> list[dict]:
         arr = (SchedBatch * self._nb)()
         _check(self.lib.gcc_sched_batches(self._h, arr, self._nb), "gcc_sched_batches")
@@ -483,6 +517,15 @@ class Scheduler:
         out = np.zeros((n, SCHED_FEAT_STRIDE), dtype=np.uint16)
         _check(self.lib.gcc_sched_features(self._h, first, n, _ptr(out)), "gcc_sched_features")
         return out
+
+    def features_var(self, first: int, n: int) -> np.ndarray:
+        out = np.zeros((n, SCHED_FEAT_STRIDE), dtype=np.uint16)
+        _check(self.lib.gcc_sched_features_var(self._h, first, n, _ptr(out)), "gcc_sched_features_var")
+        return out
+
+    def observe_var(self, first: int, n: int, clear: bool = False):
+        _check(self.lib.gcc_sched_observe_var(self._h, first, n, 1 if clear else 0),
+               "gcc_sched_observe_var")
 
     def observe(self, first: int, n: int, clear: bool = False):
         _check(self.lib.gcc_sched_observe(self._h, first, n, 1 if clear else 0), "gcc_sched_observe")

@@ -12,12 +12,14 @@
 //   metrics + output line                include/runtime.cuh:169-214
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <map>
 #include <cstdio>
 #include <cstring>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "cc_launch.cuh"
@@ -1474,7 +1476,7 @@ int gcc_sched_create(gcc_engine *e, const gcc_sched_params *p, gcc_sched **out) 
     *out = nullptr;
     if (p->mode != GCC_SCHED_PLAIN && p->mode != GCC_SCHED_LEARNED) return GCC_EINVAL;
     if (p->explore_every < 0 || p->minibatch < 0 || p->train_steps < -1 || p->probe_rows < 0 ||
-        p->fixed_arm < 0)
+        p->fixed_arm < 0 || p->min_sched < -1)
         return GCC_EINVAL;
     if (p->minibatch > (1 << 20) || p->probe_rows > (1 << 20)) return GCC_EINVAL;
     if (!(p->lr >= 0.f) || !(p->defer_threshold >= 0.f) || p->defer_threshold >= 1.f)
@@ -1487,6 +1489,7 @@ int gcc_sched_create(gcc_engine *e, const gcc_sched_params *p, gcc_sched **out) 
     if (!s->prm.train_steps) s->prm.train_steps = 4;
     if (!s->prm.minibatch) s->prm.minibatch = 4096;
     if (!s->prm.probe_rows) s->prm.probe_rows = 4096;
+    if (!s->prm.min_sched) s->prm.min_sched = 4096;
     if (s->prm.lr == 0.f) s->prm.lr = 2e-3f;
     if (s->prm.defer_threshold == 0.f) s->prm.defer_threshold = 0.2f;
     cudaError_t ce = s->pred.init(e->dev, e->stream,
@@ -1529,6 +1532,31 @@ int gcc_sched_features(gcc_sched *s, uint64_t first, uint64_t n, uint16_t *dst) 
     if (ce == cudaSuccess && n)
         ce = cudaMemcpyAsync(dst, s->pred.feat, n * sched::kFeatStride * 2, cudaMemcpyDeviceToHost,
                              e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    return ce == cudaSuccess ? GCC_OK : s->fail(ce);
+}
+
+int gcc_sched_features_var(gcc_sched *s, uint64_t first, uint64_t n, uint16_t *dst) {
+    if (!s || (!dst && n) || n > (1ull << 20)) return GCC_EINVAL;
+    gcc_engine *e = s->e;
+    if (!e->reqs_d || first + n > e->n_var) return GCC_ESTATE;
+    cudaSetDevice(e->dev);
+    cudaError_t ce = s->pred.reserve(n);
+    if (ce == cudaSuccess) ce = s->pred.features_var(e->tx_off_d, e->reqs_d, first, n, s->pred.feat);
+    if (ce == cudaSuccess && n)
+        ce = cudaMemcpyAsync(dst, s->pred.feat, n * sched::kFeatStride * 2, cudaMemcpyDeviceToHost,
+                             e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    return ce == cudaSuccess ? GCC_OK : s->fail(ce);
+}
+
+int gcc_sched_observe_var(gcc_sched *s, uint64_t first, uint64_t n, int32_t clear) {
+    if (!s) return GCC_EINVAL;
+    gcc_engine *e = s->e;
+    if (n && (!e->reqs_d || first + n > e->n_var)) return GCC_ESTATE;
+    cudaSetDevice(e->dev);
+    cudaError_t ce = clear ? s->pred.clear_freq() : cudaSuccess;
+    if (ce == cudaSuccess) ce = s->pred.observe_var(e->tx_off_d, e->reqs_d, first, n);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
     return ce == cudaSuccess ? GCC_OK : s->fail(ce);
 }
@@ -1620,288 +1648,331 @@ int gcc_sched_batches(gcc_sched *s, gcc_sched_batch *dst, uint64_t n) {
     return GCC_OK;
 }
 
-int gcc_sched_run(gcc_sched *sc, const gcc_run_params *rp, gcc_sched_result *out) {
-    cudaGetLastError();
-    if (!sc || !rp || !out) return GCC_EINVAL;
-    memset(out, 0, sizeof(*out));
+}  // extern "C"
+
+namespace {
+
+// Per-run state of the scheduled driver, shared by gcc_sched_run (fixed
+// batches of 16-request records) and gcc_serve (admitted batches of
+// variable-length transactions).
+struct SchedRun {
+    gcc_sched *sc = nullptr;
+    gcc_engine *e = nullptr;
+    const gcc_run_params *rp = nullptr;
+    int s = 0, G = 0, block = 0, occ_main = 0, occ_wd = 0;
+    bool var = false, learned = false;
+    uint64_t user_grid = 0, batch_index = 0;
+    KParams base;
+    cudaEvent_t ev0, ev1, evk0, evk1, evt0, evt1, evp1, evq;
+    double tot_ms = 0, proc_ms = 0, pred_ms = 0, train_ms = 0, probe_ms = 0, sched_ms = 0;
+    uint64_t probe_c = 0, probe_a = 0, sched_c = 0, sched_a = 0;
+    unsigned long long prev[2] = {0, 0};
+    uint64_t launches0 = 0;
+    std::vector<uint8_t> ylab;
+};
+
+// Validate the run, size the buffers for batches of up to max_batch
+// transactions, reset the counters.
+int sched_setup(SchedRun &R, gcc_sched *sc, const gcc_run_params *rp, bool var, uint64_t max_batch) {
     gcc_engine *e = sc->e;
+    R.sc = sc;
+    R.e = e;
+    R.rp = rp;
+    R.var = var;
     const int s = gcc_scheme_id(rp->cc_scheme);
     if (s != S_TPL_NW && s != S_TPL_WD && s != S_SILO && s != S_TICTOC) return GCC_EINVAL;
-    if (rp->warp_density < 0 || rp->warp_density > 5) return GCC_EINVAL;
+    if (rp->warp_density < (var ? 2 : 0) || rp->warp_density > 5) return GCC_EINVAL;
     if (rp->block_size < 1 || rp->block_size > 32) return GCC_EINVAL;
-    if (rp->batch_size < 1 || rp->batch_size > (1 << 20)) return GCC_EINVAL;
     if (rp->write_mode != GCC_WRITE_FIELD) return GCC_EINVAL;
-    if (rp->flags & (GCC_F_READ_LOG | GCC_F_AUTOTUNE | GCC_F_GRAPH | GCC_F_EXT_OPS)) return GCC_EINVAL;
+    if (rp->flags & (GCC_F_READ_LOG | GCC_F_AUTOTUNE | GCC_F_GRAPH)) return GCC_EINVAL;
+    if (!var && (rp->flags & GCC_F_EXT_OPS)) return GCC_EINVAL;
+    if (!ext_ops_allowed(e, s, rp)) return GCC_EINVAL;
     if (rp->backoff_ns < -1 || rp->backoff_ns > 100000) return GCC_EINVAL;
     if (rp->max_active < 0 || rp->starve_limit < -1) return GCC_EINVAL;
-    if (!e->txs || e->n_rec == 0) return GCC_ESTATE;
+    if (max_batch == 0 || max_batch > (1ull << 20)) return GCC_EINVAL;
     cudaSetDevice(e->dev);
-    e->n_tx = e->n_rec;
-    const bool learned = sc->prm.mode == GCC_SCHED_LEARNED;
-    const uint64_t n = e->n_tx;
-    const uint64_t batch = std::min<uint64_t>((uint64_t)rp->batch_size, n);
-    const uint64_t nb = (n + batch - 1) / batch;
-    const int G = 1 << rp->warp_density, block = rp->block_size * 32;
-    int rc;
+    R.s = s;
+    R.learned = sc->prm.mode == GCC_SCHED_LEARNED;
+    R.G = 1 << rp->warp_density;
+    R.block = rp->block_size * 32;
+    const uint64_t n = var ? e->n_var : e->n_rec;
     cudaError_t ce;
-    if ((ce = sc->pred.reserve(batch))) return sc->fail(ce);
+    if ((ce = sc->pred.reserve(max_batch))) return sc->fail(ce);
     if (sc->order_cap < n) {
         if (sc->order) cudaFree(sc->order);
         sc->order = nullptr;
         if ((ce = cudaMalloc(&sc->order, n * 4))) return sc->fail(ce);
         sc->order_cap = n;
     }
-    const uint64_t pneed = (batch + 1023) / 1024 * 3;
+    const uint64_t pneed = (max_batch + 1023) / 1024 * 3;
     if (sc->part_cap < pneed) {
         if (sc->part_scratch) cudaFree(sc->part_scratch);
         sc->part_scratch = nullptr;
         if ((ce = cudaMalloc(&sc->part_scratch, pneed * 4))) return sc->fail(ce);
         sc->part_cap = pneed;
     }
-    const int occ_main = scheme_occupancy(s, G, block);
-    const int occ_wd = scheme_occupancy(S_TPL_WD, G, block);
-    if (occ_main <= 0 || occ_wd <= 0) return GCC_EINVAL;
+    R.occ_main = var ? occupancy_var(s, R.G, R.block) : scheme_occupancy(s, R.G, R.block);
+    R.occ_wd = var ? occupancy_var(S_TPL_WD, R.G, R.block) : scheme_occupancy(S_TPL_WD, R.G, R.block);
+    if (R.occ_main <= 0 || R.occ_wd <= 0) return GCC_EINVAL;
     if (sc->policy_scheme != s) sc->set_arms(s);
-
-    KParams base = e->base_params();
-    base.write_mode = rp->write_mode;
-    base.write_seed = rp->write_seed;
-    base.flags = rp->flags;
-    base.spin_limit_ns = rp->spin_limit_ns ? rp->spin_limit_ns : 4000000000ull;
-    base.backoff_ns = rp->backoff_ns < 0 ? 0u : (rp->backoff_ns == 0 ? 512u : (uint32_t)rp->backoff_ns);
-    base.starve_limit = starve_param(rp->starve_limit);
-    const uint64_t user_grid = std::min<uint64_t>((uint64_t)occ_main * e->sm_count,
-                                                  active_grid(rp->max_active, G, block));
-
+    KParams &b = R.base;
+    b = e->base_params();
+    if (var) {
+        b.txs = nullptr;
+        b.tx_off = e->tx_off_d;
+        b.reqs = e->reqs_d;
+        b.n_tx = (uint32_t)e->n_var;
+        b.slot_ops = kMaxVarOps;
+        b.ext_ops = (rp->flags & GCC_F_EXT_OPS) ? 1u : 0u;
+    }
+    b.write_mode = rp->write_mode;
+    b.write_seed = rp->write_seed;
+    b.flags = rp->flags;
+    b.spin_limit_ns = rp->spin_limit_ns ? rp->spin_limit_ns : 4000000000ull;
+    b.backoff_ns = rp->backoff_ns < 0 ? 0u : (rp->backoff_ns == 0 ? 512u : (uint32_t)rp->backoff_ns);
+    b.starve_limit = starve_param(rp->starve_limit);
+    R.user_grid = std::min<uint64_t>((uint64_t)R.occ_main * e->sm_count,
+                                     active_grid(rp->max_active, R.G, R.block));
+    int rc;
     if ((rc = e->ensure_events(8))) return rc;
-    cudaEvent_t ev0 = e->events[0], ev1 = e->events[1], evk0 = e->events[2], evk1 = e->events[3],
-                evt0 = e->events[4], evt1 = e->events[5], evp1 = e->events[6], evq = e->events[7];
-    cudaStream_t st = e->stream;
-    if ((ce = cudaMemsetAsync(e->ctr, 0, sizeof(Counters), st))) return sc->fail(ce);
-    sc->batches.assign(nb, gcc_sched_batch{});
-    const uint64_t launches0 = e->kernel_launches;
-    double tot_ms = 0, proc_ms = 0, pred_ms = 0, train_ms = 0, probe_ms = 0, sched_ms = 0;
-    uint64_t probe_c = 0, probe_a = 0, sched_c = 0, sched_a = 0;
-    unsigned long long prev[2] = {0, 0};
-    std::vector<uint8_t> ylab;
+    R.ev0 = e->events[0]; R.ev1 = e->events[1]; R.evk0 = e->events[2]; R.evk1 = e->events[3];
+    R.evt0 = e->events[4]; R.evt1 = e->events[5]; R.evp1 = e->events[6]; R.evq = e->events[7];
+    if ((ce = cudaMemsetAsync(e->ctr, 0, sizeof(Counters), e->stream))) return sc->fail(ce);
+    R.launches0 = e->kernel_launches;
+    e->n_tx = n;
+    return GCC_OK;
+}
 
-    auto launch = [&](int sch, uint64_t bst, uint64_t bn, const uint32_t *order,
+// One batch (transactions bst .. bst + bn - 1) under the schedule; fills rec.
+int sched_batch(SchedRun &R, uint64_t bst, uint64_t bn, gcc_sched_batch &rec) {
+    gcc_sched *sc = R.sc;
+    gcc_engine *e = R.e;
+    const gcc_run_params *rp = R.rp;
+    const int s = R.s, G = R.G, block = R.block;
+    cudaStream_t st = e->stream;
+    cudaError_t ce;
+    auto launch = [&](int sch, uint64_t b0, uint64_t cnt, const uint32_t *order,
                       uint64_t grid_cap) -> cudaError_t {
-        KParams q = base;
-        q.batch_st = (uint32_t)bst;
-        q.batch_n = (uint32_t)bn;
+        KParams q = R.base;
+        q.batch_st = (uint32_t)b0;
+        q.batch_n = (uint32_t)cnt;
         q.order = order;
         q.wait_die = sch == S_TPL_WD ? 1u : 0u;
         k_batch_prep<<<1, 32, 0, st>>>(e->ctr, 0);
         cudaError_t c = cudaGetLastError();
         if (c != cudaSuccess) return c;
-        const uint64_t want = (bn * (uint64_t)G + block - 1) / block;
+        const uint64_t want = (cnt * (uint64_t)G + block - 1) / block;
         const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, grid_cap));
         e->kernel_launches += 2;
-        return launch_scheme_kernel(sch, G, grid, block, q, st);
+        return R.var ? launch_var(sch, G, grid, block, q, st)
+                     : launch_scheme_kernel(sch, G, grid, block, q, st);
     };
     auto counters = [&](unsigned long long *ca) -> cudaError_t {
         cudaError_t c = cudaMemcpyAsync(ca, &e->ctr->committed, 16, cudaMemcpyDeviceToHost, st);
         return c == cudaSuccess ? cudaStreamSynchronize(st) : c;
     };
-
     // one part of a batch under an arm: plain ordering (one launch), or the
     // predicted-safe transactions at full concurrency then the deferred ones
     // with the arm's in-flight cap
     auto run_part = [&](const SchedArm &a, uint64_t st0, uint64_t cnt, uint32_t n_low) -> cudaError_t {
         if (!cnt) return cudaSuccess;
-        if (!a.defer) return launch(s, st0, cnt, nullptr, user_grid);
+        if (!a.defer) return launch(s, st0, cnt, nullptr, R.user_grid);
         cudaError_t c = cudaSuccess;
-        if (n_low) c = launch(s, st0, n_low, sc->order, user_grid);
+        if (n_low) c = launch(s, st0, n_low, sc->order, R.user_grid);
         if (c == cudaSuccess && cnt > n_low) {
             const int sch2 = a.wd ? S_TPL_WD : s;
-            const int occ2 = a.wd ? occ_wd : occ_main;
+            const int occ2 = a.wd ? R.occ_wd : R.occ_main;
             const uint64_t cap_grid = std::min<uint64_t>((uint64_t)occ2 * e->sm_count,
                                                          active_grid((int32_t)a.cap, G, block));
             c = launch(sch2, st0 + n_low, cnt - n_low, sc->order, cap_grid);
         }
         return c;
     };
-
-    for (uint64_t b = 0; b < nb; ++b) {
-        const uint64_t bst = b * batch, bn = std::min<uint64_t>(batch, n - bst);
-        gcc_sched_batch &rec = sc->batches[b];
-        const uint64_t probe = (learned && b % (uint64_t)sc->prm.explore_every == 0)
-                                   ? std::min<uint64_t>(bn, (uint64_t)sc->prm.probe_rows) : 0;
-        const uint64_t rst = bst + probe, rn = bn - probe;
-        rec.kind = learned ? 1u : 0u;
-        rec.probe = (uint32_t)probe;
-        if ((ce = cudaEventRecord(ev0, st))) return sc->fail(ce);
-        if (b == 0 || !(rp->flags & GCC_F_NO_RESET))
-            if ((ce = cudaMemsetAsync(e->meta, 0, e->rows * 8, st))) return sc->fail(ce);
-        // the part after the probe runs under the bucket's incumbent arm; when
-        // the bucket has a candidate, its second half runs under the
-        // candidate instead, so both arms meet the same workload
-        int arm_i = 0, cand = -1;
-        uint64_t seg_n[2] = {rn, 0};
-        uint32_t n_low[2] = {(uint32_t)rn, 0};
-        float bpred_ms = 0;
-        if (learned) {
-            ce = sc->pred.features(e->txs, bst, bn, sc->pred.feat);
-            if (ce == cudaSuccess) ce = sc->pred.forward(sc->pred.feat, bn, sc->pred.p);
-            e->kernel_launches += 4;  // features, 2 GEMMs + head
-            // the bucket comes from the mean prediction over the batch
-            float hsums[4] = {0.f, 0.f, 0.f, 0.f};
-            if (ce == cudaSuccess) {
-                ce = sched::partition(sc->pred.p, bst, bn, sc->prm.defer_threshold, sc->order + bst,
-                                      sc->counts, sc->sums, sc->part_scratch, st);
-                e->kernel_launches += 3;
-            }
-            if (ce == cudaSuccess) ce = cudaMemcpyAsync(hsums, sc->sums, 8, cudaMemcpyDeviceToHost, st);
-            if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
-            if (ce != cudaSuccess) return sc->fail(ce);
-            rec.pred_mean = hsums[0] / (float)bn;
-            rec.bucket = (uint32_t)contention_bucket(rec.pred_mean);
-            if (sc->prm.fixed_arm > 0) {
-                arm_i = std::min<int>(sc->prm.fixed_arm - 1, (int)sc->arms.size() - 1);
-            } else {
-                arm_i = sc->inc;
-                cand = rn >= 2048 ? sc->candidate(rec.pred_mean) : -1;
-            }
-            if (cand >= 0) {
-                seg_n[0] = rn / 2;
-                seg_n[1] = rn - seg_n[0];
-            }
-            // risk partition of each part (positions keep their part)
-            uint64_t off = rst;
-            for (int k = 0; k < 2 && ce == cudaSuccess; ++k) {
-                if (!seg_n[k]) continue;
-                ce = sched::partition(sc->pred.p + (off - bst), off, seg_n[k], sc->prm.defer_threshold,
-                                      sc->order + off, sc->counts + k, sc->sums + 2 * k,
-                                      sc->part_scratch, st);
-                e->kernel_launches += 3;
-                off += seg_n[k];
-            }
-            if (ce == cudaSuccess) ce = cudaMemcpyAsync(n_low, sc->counts, 8, cudaMemcpyDeviceToHost, st);
-            if (ce == cudaSuccess) ce = cudaEventRecord(evp1, st);
-            if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
-            if (ce != cudaSuccess) return sc->fail(ce);
-            if (!seg_n[1]) n_low[1] = 0;
-            cudaEventElapsedTime(&bpred_ms, ev0, evp1);
-            pred_ms += bpred_ms;
+    const bool learned = R.learned && (sc->prm.min_sched < 0 || bn >= (uint64_t)sc->prm.min_sched);
+    const uint64_t b = R.batch_index++;
+    const uint64_t probe = (learned && b % (uint64_t)sc->prm.explore_every == 0)
+                               ? std::min<uint64_t>(bn, (uint64_t)sc->prm.probe_rows) : 0;
+    const uint64_t rst = bst + probe, rn = bn - probe;
+    rec = gcc_sched_batch{};
+    rec.kind = learned ? 1u : 0u;
+    rec.probe = (uint32_t)probe;
+    if ((ce = cudaEventRecord(R.ev0, st))) return sc->fail(ce);
+    if (b == 0 || !(rp->flags & GCC_F_NO_RESET))
+        if ((ce = cudaMemsetAsync(e->meta, 0, e->rows * 8, st))) return sc->fail(ce);
+    // the part after the probe runs under the incumbent arm; when there is a
+    // candidate, its second half runs under the candidate instead, so both
+    // arms meet the same workload
+    int arm_i = 0, cand = -1;
+    uint64_t seg_n[2] = {rn, 0};
+    uint32_t n_low[2] = {(uint32_t)rn, 0};
+    float bpred_ms = 0;
+    if (learned) {
+        ce = R.var ? sc->pred.features_var(e->tx_off_d, e->reqs_d, bst, bn, sc->pred.feat)
+                   : sc->pred.features(e->txs, bst, bn, sc->pred.feat);
+        if (ce == cudaSuccess) ce = sc->pred.forward(sc->pred.feat, bn, sc->pred.p);
+        e->kernel_launches += 4;  // features, 2 GEMMs + head
+        float hsums[4] = {0.f, 0.f, 0.f, 0.f};
+        if (ce == cudaSuccess) {
+            ce = sched::partition(sc->pred.p, bst, bn, sc->prm.defer_threshold, sc->order + bst,
+                                  sc->counts, sc->sums, sc->part_scratch, st);
+            e->kernel_launches += 3;
         }
-        const SchedArm arm = sc->arms[arm_i];
-        rec.arm = (uint32_t)arm_i;
-        rec.explored = cand >= 0 ? (uint32_t)cand + 1u : 0u;
-        rec.in_flight_cap = arm.defer ? arm.cap : 0u;
-        rec.wait_die = arm.defer ? arm.wd : 0u;
-        rec.deferred = (arm.defer ? seg_n[0] - n_low[0] : 0u) +
-                       (cand >= 0 && sc->arms[cand].defer ? seg_n[1] - n_low[1] : 0u);
-
-        // the probe: plain ordering at full concurrency, labels for training
-        unsigned long long c_probe[2] = {prev[0], prev[1]};
-        if (probe) {
-            if ((ce = launch(s, bst, probe, nullptr, user_grid))) return sc->fail(ce);
-            if ((ce = cudaEventRecord(evq, st))) return sc->fail(ce);
-            if ((ce = counters(c_probe))) return sc->fail(ce);
-            float qms = 0;
-            cudaEventElapsedTime(&qms, learned ? evp1 : ev0, evq);
-            probe_ms += qms;
-            probe_c += c_probe[0] - prev[0];
-            probe_a += c_probe[1] - prev[1];
-        }
-        if ((ce = cudaEventRecord(evk0, st))) return sc->fail(ce);
-        ce = run_part(arm, rst, seg_n[0], n_low[0]);
-        if (ce == cudaSuccess) ce = cudaEventRecord(evt1, st);  // end of the first part
-        if (ce == cudaSuccess && cand >= 0) ce = run_part(sc->arms[cand], rst + seg_n[0], seg_n[1], n_low[1]);
-        if (ce == cudaSuccess) ce = cudaEventRecord(evk1, st);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(hsums, sc->sums, 8, cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
         if (ce != cudaSuccess) return sc->fail(ce);
-        float part_ms[2] = {0.f, 0.f};
+        rec.pred_mean = hsums[0] / (float)bn;
+        rec.bucket = (uint32_t)contention_bucket(rec.pred_mean);
+        if (sc->prm.fixed_arm > 0) {
+            arm_i = std::min<int>(sc->prm.fixed_arm - 1, (int)sc->arms.size() - 1);
+        } else {
+            arm_i = sc->inc;
+            cand = rn >= 2048 ? sc->candidate(rec.pred_mean) : -1;
+        }
         if (cand >= 0) {
-            if ((ce = cudaEventSynchronize(evk1))) return sc->fail(ce);
-            cudaEventElapsedTime(&part_ms[0], evk0, evt1);
-            cudaEventElapsedTime(&part_ms[1], evt1, evk1);
+            seg_n[0] = rn / 2;
+            seg_n[1] = rn - seg_n[0];
         }
-
-        if (probe && sc->prm.train_steps > 0) {
-            // labels of the probe, the loss of the predictions made before
-            // training on them, then Adam steps
-            ce = cudaEventRecord(evt0, st);
-            if (ce == cudaSuccess) ce = sched::abort_labels(e->tx_aborts, bst, probe, sc->pred.labels, st);
-            e->kernel_launches += 1;
-            ylab.resize(probe);
-            if (ce == cudaSuccess)
-                ce = cudaMemcpyAsync(ylab.data(), sc->pred.labels, probe, cudaMemcpyDeviceToHost, st);
-            const uint64_t mb = std::min<uint64_t>(probe, (uint64_t)sc->prm.minibatch);
-            for (int32_t k = 0; k < sc->prm.train_steps && ce == cudaSuccess; ++k) {
-                const uint64_t off = ((uint64_t)k * mb) % probe;
-                const uint64_t rows = std::min<uint64_t>(mb, probe - off);
-                ce = sc->pred.gradient(sc->pred.feat + off * sched::kFeatStride,
-                                       sc->pred.labels + off, rows);
-                if (ce == cudaSuccess && k == 0) {
-                    float l0 = 0.f;
-                    ce = cudaMemcpyAsync(&l0, sc->pred.loss, 4, cudaMemcpyDeviceToHost, st);
-                    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
-                    rec.loss = l0 / (float)rows;
-                }
-                if (ce == cudaSuccess) ce = sc->pred.adam(sc->prm.lr);
-                e->kernel_launches += 13;
-            }
-            if (ce == cudaSuccess) ce = cudaEventRecord(evt1, st);
-            if (ce != cudaSuccess) return sc->fail(ce);
+        // risk partition of each part (positions keep their part)
+        uint64_t off = rst;
+        for (int k = 0; k < 2 && ce == cudaSuccess; ++k) {
+            if (!seg_n[k]) continue;
+            ce = sched::partition(sc->pred.p + (off - bst), off, seg_n[k], sc->prm.defer_threshold,
+                                  sc->order + off, sc->counts + k, sc->sums + 2 * k,
+                                  sc->part_scratch, st);
+            e->kernel_launches += 3;
+            off += seg_n[k];
         }
-        if (learned) {
-            if ((ce = sc->pred.observe(e->txs, bst, bn))) return sc->fail(ce);
-            e->kernel_launches += 2;
-        }
-        if ((ce = cudaEventRecord(ev1, st))) return sc->fail(ce);
-        unsigned long long ca[2];
-        if ((ce = counters(ca))) return sc->fail(ce);
-        float ms = 0, kms = 0;
-        cudaEventElapsedTime(&ms, ev0, ev1);
-        cudaEventElapsedTime(&kms, evk0, evk1);
-        if (probe && sc->prm.train_steps > 0) {
-            float tms = 0;
-            cudaEventElapsedTime(&tms, evt0, evt1);
-            train_ms += tms;
-            uint64_t pos = 0;
-            for (uint8_t v : ylab) pos += v;
-            rec.label_mean = (float)pos / (float)probe;
-        }
-        rec.ms = ms;
-        rec.committed = ca[0] - prev[0];
-        rec.aborts = ca[1] - prev[1];
-        tot_ms += ms;
-        proc_ms += kms;
-        sched_ms += kms;
-        sched_c += ca[0] - c_probe[0];
-        sched_a += ca[1] - c_probe[1];
-        prev[0] = ca[0];
-        prev[1] = ca[1];
-        // the comparison: the candidate replaces the incumbent when its half
-        // ran at least 3% faster per transaction
-        if (cand >= 0) {
-            sc->tried[cand] = 1;
-            const double t_inc = part_ms[0] / (double)seg_n[0];
-            const double t_cand = part_ms[1] / (double)seg_n[1];
-            if (t_cand < 0.97 * t_inc) {
-                sc->tried[arm_i] = 1;
-                sc->inc = cand;
-            }
-        }
-        unsigned err = 0;
-        if (cudaMemcpy(&err, &e->ctr->err, 4, cudaMemcpyDeviceToHost) == cudaSuccess && err) break;
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(n_low, sc->counts, 8, cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess) ce = cudaEventRecord(R.evp1, st);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+        if (ce != cudaSuccess) return sc->fail(ce);
+        if (!seg_n[1]) n_low[1] = 0;
+        cudaEventElapsedTime(&bpred_ms, R.ev0, R.evp1);
+        R.pred_ms += bpred_ms;
     }
+    const SchedArm arm = sc->arms[arm_i];
+    rec.arm = (uint32_t)arm_i;
+    rec.explored = cand >= 0 ? (uint32_t)cand + 1u : 0u;
+    rec.in_flight_cap = arm.defer ? arm.cap : 0u;
+    rec.wait_die = arm.defer ? arm.wd : 0u;
+    rec.deferred = (arm.defer ? seg_n[0] - n_low[0] : 0u) +
+                   (cand >= 0 && sc->arms[cand].defer ? seg_n[1] - n_low[1] : 0u);
 
+    // the probe: plain ordering at full concurrency, labels for training
+    unsigned long long c_probe[2] = {R.prev[0], R.prev[1]};
+    if (probe) {
+        if ((ce = launch(s, bst, probe, nullptr, R.user_grid))) return sc->fail(ce);
+        if ((ce = cudaEventRecord(R.evq, st))) return sc->fail(ce);
+        if ((ce = counters(c_probe))) return sc->fail(ce);
+        float qms = 0;
+        cudaEventElapsedTime(&qms, R.evp1, R.evq);
+        R.probe_ms += qms;
+        R.probe_c += c_probe[0] - R.prev[0];
+        R.probe_a += c_probe[1] - R.prev[1];
+    }
+    if ((ce = cudaEventRecord(R.evk0, st))) return sc->fail(ce);
+    ce = run_part(arm, rst, seg_n[0], n_low[0]);
+    if (ce == cudaSuccess) ce = cudaEventRecord(R.evt1, st);  // end of the first part
+    if (ce == cudaSuccess && cand >= 0) ce = run_part(sc->arms[cand], rst + seg_n[0], seg_n[1], n_low[1]);
+    if (ce == cudaSuccess) ce = cudaEventRecord(R.evk1, st);
+    if (ce != cudaSuccess) return sc->fail(ce);
+    float part_ms[2] = {0.f, 0.f};
+    if (cand >= 0) {
+        if ((ce = cudaEventSynchronize(R.evk1))) return sc->fail(ce);
+        cudaEventElapsedTime(&part_ms[0], R.evk0, R.evt1);
+        cudaEventElapsedTime(&part_ms[1], R.evt1, R.evk1);
+    }
+    const bool train = probe && sc->prm.train_steps > 0;
+    if (train) {
+        // labels of the probe, the loss of the predictions made before
+        // training on them, then Adam steps
+        ce = cudaEventRecord(R.evt0, st);
+        if (ce == cudaSuccess) ce = sched::abort_labels(e->tx_aborts, bst, probe, sc->pred.labels, st);
+        e->kernel_launches += 1;
+        R.ylab.resize(probe);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(R.ylab.data(), sc->pred.labels, probe, cudaMemcpyDeviceToHost, st);
+        const uint64_t mb = std::min<uint64_t>(probe, (uint64_t)sc->prm.minibatch);
+        for (int32_t k = 0; k < sc->prm.train_steps && ce == cudaSuccess; ++k) {
+            const uint64_t off = ((uint64_t)k * mb) % probe;
+            const uint64_t rows = std::min<uint64_t>(mb, probe - off);
+            ce = sc->pred.gradient(sc->pred.feat + off * sched::kFeatStride, sc->pred.labels + off, rows);
+            if (ce == cudaSuccess && k == 0) {
+                float l0 = 0.f;
+                ce = cudaMemcpyAsync(&l0, sc->pred.loss, 4, cudaMemcpyDeviceToHost, st);
+                if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+                rec.loss = l0 / (float)rows;
+            }
+            if (ce == cudaSuccess) ce = sc->pred.adam(sc->prm.lr);
+            e->kernel_launches += 13;
+        }
+        if (ce == cudaSuccess) ce = cudaEventRecord(R.evt1, st);
+        if (ce != cudaSuccess) return sc->fail(ce);
+    }
+    if (learned) {
+        ce = R.var ? sc->pred.observe_var(e->tx_off_d, e->reqs_d, bst, bn)
+                   : sc->pred.observe(e->txs, bst, bn);
+        if (ce != cudaSuccess) return sc->fail(ce);
+        e->kernel_launches += 2;
+    }
+    if ((ce = cudaEventRecord(R.ev1, st))) return sc->fail(ce);
+    unsigned long long ca[2];
+    if ((ce = counters(ca))) return sc->fail(ce);
+    float ms = 0, kms = 0;
+    cudaEventElapsedTime(&ms, R.ev0, R.ev1);
+    cudaEventElapsedTime(&kms, R.evk0, R.evk1);
+    if (train) {
+        float tms = 0;
+        cudaEventElapsedTime(&tms, R.evt0, R.evt1);
+        R.train_ms += tms;
+        uint64_t pos = 0;
+        for (uint8_t v : R.ylab) pos += v;
+        rec.label_mean = (float)pos / (float)probe;
+    }
+    rec.ms = ms;
+    rec.committed = ca[0] - R.prev[0];
+    rec.aborts = ca[1] - R.prev[1];
+    R.tot_ms += ms;
+    R.proc_ms += kms;
+    R.sched_ms += kms;
+    R.sched_c += ca[0] - c_probe[0];
+    R.sched_a += ca[1] - c_probe[1];
+    R.prev[0] = ca[0];
+    R.prev[1] = ca[1];
+    // the comparison: the candidate replaces the incumbent when its half
+    // ran at least 3% faster per transaction
+    if (cand >= 0) {
+        sc->tried[cand] = 1;
+        const double t_inc = part_ms[0] / (double)seg_n[0];
+        const double t_cand = part_ms[1] / (double)seg_n[1];
+        if (t_cand < 0.97 * t_inc) {
+            sc->tried[arm_i] = 1;
+            sc->inc = cand;
+        }
+    }
+    unsigned err = 0;
+    if (cudaMemcpy(&err, &e->ctr->err, 4, cudaMemcpyDeviceToHost) == cudaSuccess && err) return (int)err;
+    return GCC_OK;
+}
+
+// Totals of the run into out (gcc_result and the scheduler's fields).
+int sched_finish(SchedRun &R, uint64_t n, uint64_t nb, gcc_sched_result *out) {
+    gcc_sched *sc = R.sc;
+    gcc_engine *e = R.e;
     Counters hc;
-    ce = cudaMemcpy(&hc, e->ctr, sizeof(Counters), cudaMemcpyDeviceToHost);
+    cudaError_t ce = cudaMemcpy(&hc, e->ctr, sizeof(Counters), cudaMemcpyDeviceToHost);
     if (ce != cudaSuccess) return sc->fail(ce);
     e->have_run = true;
-    e->last_kernel_ms = proc_ms;
+    e->last_kernel_ms = R.proc_ms;
     e->last_launches = nb;
     gcc_result *r = &out->run;
     r->committed = hc.committed;
     r->aborts = hc.aborts;
-    r->pre_s = (pred_ms + train_ms) / 1000.0;
-    r->proc_s = (proc_ms + probe_ms) / 1000.0;
-    r->tot_s = tot_ms / 1000.0;
-    r->tx_per_s = tot_ms > 0 ? (double)hc.committed * 1000.0 / tot_ms : 0.0;
-    const double inv = 1.0 / ((double)n * (double)e->clock_khz);
+    r->pre_s = (R.pred_ms + R.train_ms) / 1000.0;
+    r->proc_s = (R.proc_ms + R.probe_ms) / 1000.0;
+    r->tot_s = R.tot_ms / 1000.0;
+    r->tx_per_s = R.tot_ms > 0 ? (double)hc.committed * 1000.0 / R.tot_ms : 0.0;
+    const double inv = 1.0 / ((double)std::max<uint64_t>(1, n) * (double)e->clock_khz);
     r->ts_d = hc.ts_cycles * inv;
     r->wait_d = hc.wait_cycles * inv;
     r->abort_d = hc.abort_cycles * inv;
@@ -1909,7 +1980,7 @@ int gcc_sched_run(gcc_sched *sc, const gcc_run_params *rp, gcc_sched_result *out
     r->tot_d = hc.tot_cycles * inv;
     r->idx_d = hc.idx_cycles * inv;
     r->batches = nb;
-    r->kernel_launches = e->kernel_launches - launches0;
+    r->kernel_launches = e->kernel_launches - R.launches0;
     r->max_attempts = hc.max_attempts;
     r->err_site = hc.err_where;
     uint64_t total = 0;
@@ -1935,14 +2006,133 @@ int gcc_sched_run(gcc_sched *sc, const gcc_run_params *rp, gcc_sched_result *out
         out->deferred += rec.deferred;
         if (rec.probe && sc->prm.train_steps > 0) out->last_loss = rec.loss;
     }
-    out->probe_tx_per_s = probe_ms > 0 ? probe_c * 1000.0 / probe_ms : 0.0;
-    out->sched_tx_per_s = sched_ms > 0 ? sched_c * 1000.0 / sched_ms : 0.0;
-    out->probe_abort_rate = probe_c + probe_a ? (double)probe_a / (double)(probe_c + probe_a) : 0.0;
-    out->sched_abort_rate = sched_c + sched_a ? (double)sched_a / (double)(sched_c + sched_a) : 0.0;
-    out->predict_ms = pred_ms;
-    out->train_ms = train_ms;
+    out->probe_tx_per_s = R.probe_ms > 0 ? R.probe_c * 1000.0 / R.probe_ms : 0.0;
+    out->sched_tx_per_s = R.sched_ms > 0 ? R.sched_c * 1000.0 / R.sched_ms : 0.0;
+    out->probe_abort_rate = R.probe_c + R.probe_a ? (double)R.probe_a / (double)(R.probe_c + R.probe_a) : 0.0;
+    out->sched_abort_rate = R.sched_c + R.sched_a ? (double)R.sched_a / (double)(R.sched_c + R.sched_a) : 0.0;
+    out->predict_ms = R.pred_ms;
+    out->train_ms = R.train_ms;
     if (hc.err) return (int)hc.err;
     if (hc.committed != n) return GCC_ESTATE;
+    return GCC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gcc_sched_run(gcc_sched *sc, const gcc_run_params *rp, gcc_sched_result *out) {
+    cudaGetLastError();
+    if (!sc || !rp || !out) return GCC_EINVAL;
+    memset(out, 0, sizeof(*out));
+    gcc_engine *e = sc->e;
+    if (!e->txs || e->n_rec == 0) return GCC_ESTATE;
+    if (rp->batch_size < 1 || rp->batch_size > (1 << 20)) return GCC_EINVAL;
+    const uint64_t n = e->n_rec;
+    const uint64_t batch = std::min<uint64_t>((uint64_t)rp->batch_size, n);
+    const uint64_t nb = (n + batch - 1) / batch;
+    SchedRun R;
+    int rc = sched_setup(R, sc, rp, false, batch);
+    if (rc) return rc;
+    sc->batches.assign(nb, gcc_sched_batch{});
+    for (uint64_t b = 0; b < nb; ++b) {
+        const uint64_t bst = b * batch, bn = std::min<uint64_t>(batch, n - bst);
+        rc = sched_batch(R, bst, bn, sc->batches[b]);
+        if (rc) break;
+    }
+    const int rc2 = sched_finish(R, n, nb, out);
+    return rc ? rc : rc2;
+}
+
+int gcc_serve(gcc_sched *sc, const gcc_run_params *rp, const gcc_serve_params *sp,
+              gcc_serve_result *out) {
+    cudaGetLastError();
+    if (!sc || !rp || !sp || !out) return GCC_EINVAL;
+    memset(out, 0, sizeof(*out));
+    gcc_engine *e = sc->e;
+    if (!e->n_var || !e->reqs_d) return GCC_ESTATE;
+    if (!(sp->rate_tps > 0.0) || sp->max_batch < 0 || sp->min_batch < 0 || !(sp->max_wait_us >= 0.0))
+        return GCC_EINVAL;
+    const uint64_t n = e->n_var;
+    cudaSetDevice(e->dev);
+    // admission cap: the caller's, else what half the free device memory
+    // holds at the scheduler's per-transaction footprint (activations,
+    // features, probabilities, labels, partition scratch)
+    uint64_t cap = sp->max_batch ? (uint64_t)sp->max_batch : 0;
+    if (!cap) {
+        size_t fr = 0, tot = 0;
+        cudaError_t ce = cudaMemGetInfo(&fr, &tot);
+        if (ce != cudaSuccess) return e->fail_cuda(ce);
+        const uint64_t per_tx = 4ull * sched::kHid * 4 + sched::kFeatStride * 2 + 16;
+        cap = (uint64_t)(fr / 2) / per_tx;
+    }
+    cap = std::max<uint64_t>(1, std::min<uint64_t>({cap, 1ull << 20, n}));
+    SchedRun R;
+    int rc = sched_setup(R, sc, rp, true, cap);
+    if (rc) return rc;
+    // Poisson arrivals: exponential gaps from a counter-based hash
+    std::vector<double> arrive(n);
+    double t = 0.0;
+    for (uint64_t i = 0; i < n; ++i) {
+        const double u = ((double)(hash3(sp->seed, i, 0x415252ull) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+        t += -std::log(u) / sp->rate_tps;
+        arrive[i] = t;
+    }
+    const uint64_t min_b = sp->min_batch ? (uint64_t)sp->min_batch : 1;
+    const double max_wait = (sp->max_wait_us > 0.0 ? sp->max_wait_us : 200.0) * 1e-6;
+    std::vector<double> lat(n);
+    sc->batches.clear();
+    const auto t0 = std::chrono::steady_clock::now();
+    auto now = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
+    uint64_t next = 0, arrived = 0;
+    double busy = 0.0;
+    while (next < n) {
+        const double tn = now();
+        while (arrived < n && arrive[arrived] <= tn) ++arrived;
+        const uint64_t waiting = arrived - next;
+        if (waiting == 0 || (waiting < min_b && tn - arrive[next] < max_wait && arrived < n)) {
+            // idle until the next arrival (or the wait bound), sleeping when
+            // that is far enough away
+            const double until = waiting == 0 ? arrive[next] : arrive[next] + max_wait;
+            const double dt = until - tn;
+            if (dt > 200e-6)
+                std::this_thread::sleep_for(std::chrono::microseconds((int64_t)((dt - 100e-6) * 1e6)));
+            continue;
+        }
+        const uint64_t bn = std::min<uint64_t>(waiting, cap);
+        sc->batches.push_back(gcc_sched_batch{});
+        const double b0 = now();
+        rc = sched_batch(R, next, bn, sc->batches.back());
+        const double b1 = now();
+        busy += b1 - b0;
+        if (rc) break;
+        for (uint64_t i = next; i < next + bn; ++i) lat[i] = b1 - arrive[i];
+        next += bn;
+    }
+    const double wall = now();
+    gcc_sched_result sr;
+    memset(&sr, 0, sizeof(sr));
+    const int rc2 = sched_finish(R, rc ? next : n, sc->batches.size(), &sr);
+    if (rc) return rc;
+    if (rc2) return rc2;
+    std::vector<double> ls(lat.begin(), lat.begin() + next);
+    std::sort(ls.begin(), ls.end());
+    auto q = [&](double f) {
+        return ls.empty() ? 0.0 : ls[std::min<size_t>(ls.size() - 1, (size_t)(f * ls.size()))] * 1e6;
+    };
+    out->committed = sr.run.committed;
+    out->aborts = sr.run.aborts;
+    out->batches = sc->batches.size();
+    out->admit_cap = cap;
+    out->offered_tps = n / arrive[n - 1];
+    out->tx_per_s = wall > 0 ? sr.run.committed / wall : 0.0;
+    out->device_tx_per_s = sr.run.tx_per_s;
+    out->lat_p50_us = q(0.50);
+    out->lat_p99_us = q(0.99);
+    out->lat_max_us = ls.empty() ? 0.0 : ls.back() * 1e6;
+    out->mean_batch = out->batches ? (double)n / (double)out->batches : 0.0;
+    out->busy_frac = wall > 0 ? busy / wall : 0.0;
+    out->sched_abort_rate = sr.sched_abort_rate;
     return GCC_OK;
 }
 

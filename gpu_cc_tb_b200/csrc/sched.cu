@@ -65,6 +65,66 @@ __global__ void k_features(const gcc_ycsb_tx *__restrict__ txs, uint64_t first, 
     }
 }
 
+// Variable-length transactions: the half-warp walks the requests in chunks
+// of 16 (lane l holds request 16c + l of chunk c).
+__global__ void k_features_var(const uint32_t *__restrict__ tx_off,
+                               const gcc_ycsb_req *__restrict__ reqs, uint64_t first, uint64_t n,
+                               const uint32_t *__restrict__ freq, uint16_t *__restrict__ out) {
+    const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t t = gt >> 4;
+    const unsigned l = threadIdx.x & 15u;
+    const bool live = t < n;
+    uint32_t beg = 0, cnt = 0;
+    if (live) {
+        beg = __ldg(tx_off + first + t);
+        cnt = __ldg(tx_off + first + t + 1) - beg;
+    }
+    // chunks of the longest transaction of the warp's two half-warps
+    const uint32_t chunks = __reduce_max_sync(0xFFFFFFFFu, (cnt + 15u) / 16u);
+    unsigned c0 = 0, c1 = 0, c2 = 0, c3 = 0, wsum = 0, hsum = 0;
+    for (uint32_t c = 0; c < chunks; ++c) {
+        const uint32_t i = 16u * c + l;
+        unsigned bin = 64u;
+        if (live && i < cnt) {
+            const int2 rq = *(const int2 *)(reqs + beg + i);
+            const uint32_t key = (uint32_t)rq.y;
+            bin = sketch_bin(key);
+            wsum += rq.x > 0 ? 0u : 1u;
+            hsum += heat(__ldg(freq + freq_slot(key)));
+        }
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const unsigned b = __shfl_sync(0xFFFFFFFFu, bin, (int)((threadIdx.x & 16u) | (unsigned)k));
+            c0 += b == 4u * l;
+            c1 += b == 4u * l + 1u;
+            c2 += b == 4u * l + 2u;
+            c3 += b == 4u * l + 3u;
+        }
+    }
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) {
+        wsum += __shfl_xor_sync(0xFFFFFFFFu, wsum, o, 16);
+        hsum += __shfl_xor_sync(0xFFFFFFFFu, hsum, o, 16);
+    }
+    if (!live) return;
+    uint16_t *row = out + t * kFeatStride;
+    const unsigned long long v = (unsigned long long)c0 | ((unsigned long long)c1 << 16) |
+                                 ((unsigned long long)c2 << 32) | ((unsigned long long)c3 << 48);
+    *(unsigned long long *)(row + 4 * l) = v;
+    if (l == 0) *(uint4 *)(row + kSketch) = make_uint4(wsum | (hsum << 16), 0u, 0u, 0u);
+}
+
+__global__ void k_freq_add_var(const uint32_t *__restrict__ tx_off,
+                               const gcc_ycsb_req *__restrict__ reqs, uint64_t first, uint64_t n,
+                               uint32_t *freq) {
+    const uint64_t t = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
+    const unsigned l = threadIdx.x & 15u;
+    if (t >= n) return;
+    const uint32_t beg = __ldg(tx_off + first + t), end = __ldg(tx_off + first + t + 1);
+    for (uint32_t i = beg + l; i < end; i += 16u)
+        atomicAdd(freq + freq_slot(reqs[i].key), 1u);
+}
+
 __global__ void k_freq_decay(uint32_t *freq) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < kFreqSize) freq[i] >>= 1;
@@ -433,6 +493,26 @@ cudaError_t Predictor::features(const gcc_ycsb_tx *txs, uint64_t first, uint64_t
     if (n == 0) return cudaSuccess;
     const uint64_t threads = n * 16;
     k_features<<<(unsigned)((threads + 255) / 256), 256, 0, stream>>>(txs, first, n, freq, out);
+    return cudaGetLastError();
+}
+
+cudaError_t Predictor::features_var(const uint32_t *tx_off, const gcc_ycsb_req *reqs,
+                                    uint64_t first, uint64_t n, uint16_t *out) {
+    if (n == 0) return cudaSuccess;
+    const uint64_t threads = n * 16;
+    k_features_var<<<(unsigned)((threads + 255) / 256), 256, 0, stream>>>(tx_off, reqs, first, n,
+                                                                          freq, out);
+    return cudaGetLastError();
+}
+
+cudaError_t Predictor::observe_var(const uint32_t *tx_off, const gcc_ycsb_req *reqs,
+                                   uint64_t first, uint64_t n) {
+    k_freq_decay<<<kFreqSize / 256, 256, 0, stream>>>(freq);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || n == 0) return e;
+    const uint64_t threads = n * 16;
+    k_freq_add_var<<<(unsigned)((threads + 255) / 256), 256, 0, stream>>>(tx_off, reqs, first, n,
+                                                                          freq);
     return cudaGetLastError();
 }
 

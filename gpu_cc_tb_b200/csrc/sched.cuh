@@ -89,8 +89,14 @@ struct Predictor {
     cudaError_t get_weights(float *host);
     // features of transactions first .. first + n - 1 into feat[0 .. n)
     cudaError_t features(const gcc_ycsb_tx *txs, uint64_t first, uint64_t n, uint16_t *out);
+    // the same for variable-length transactions (CSR: requests
+    // reqs[tx_off[t] .. tx_off[t+1]), up to 64)
+    cudaError_t features_var(const uint32_t *tx_off, const gcc_ycsb_req *reqs, uint64_t first,
+                             uint64_t n, uint16_t *out);
     // frequency table: halve every counter, then count the batch's requests
     cudaError_t observe(const gcc_ycsb_tx *txs, uint64_t first, uint64_t n);
+    cudaError_t observe_var(const uint32_t *tx_off, const gcc_ycsb_req *reqs, uint64_t first,
+                            uint64_t n);
     cudaError_t clear_freq();
     // p[0 .. n) = network(feat rows); activations stay in h1/h2
     cudaError_t forward(const uint16_t *f, uint64_t n, float *p_out);

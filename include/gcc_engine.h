@@ -402,6 +402,12 @@ typedef struct gcc_sched_params {
                                 runs arm k-1 of: plain ordering, deferral
                                 with in-flight cap 2048, 1024, 512, 256, and
                                 for 2PL wait-die deferral at 1024, 512 */
+    int32_t min_sched;       /* batches smaller than this run with plain
+                                ordering and skip the predictor (few
+                                transactions are in flight anyway, and the
+                                scheduling pass would add its latency);
+                                0 = 4096, -1 = schedule every batch */
+    int32_t reserved;
     uint64_t seed;           /* initial weights (He-uniform from this seed) */
 } gcc_sched_params;
 
@@ -450,6 +456,10 @@ int gcc_sched_features(gcc_sched *s, uint64_t first, uint64_t n, uint16_t *dst);
 /* Count records first .. first+n-1 into the frequency table (after halving
  * it), as a run does after each batch; clear = 1 zeroes it first. */
 int gcc_sched_observe(gcc_sched *s, uint64_t first, uint64_t n, int32_t clear);
+/* The same two over the loaded variable-length transactions (requests past
+ * the 16th count in the sketch, write and hot-key features alike). */
+int gcc_sched_features_var(gcc_sched *s, uint64_t first, uint64_t n, uint16_t *dst);
+int gcc_sched_observe_var(gcc_sched *s, uint64_t first, uint64_t n, int32_t clear);
 /* Parameters: gcc_sched_param_count() FP32 values, layout W1[66][128],
  * b1[128], W2[128][128], b2[128], w3[128], b3. set rounds them to BF16 for
  * compute and resets Adam. */
@@ -466,6 +476,40 @@ int gcc_sched_gradient(gcc_sched *s, const uint16_t *feat, const uint8_t *labels
  * *loss = mean loss of the last step. */
 int gcc_sched_train(gcc_sched *s, const uint16_t *feat, const uint8_t *labels, uint64_t n,
                     int32_t steps, double *loss);
+
+/* ---- Serving (no counterpart in the reference, which runs a fixed dataset
+ * in batches): the engine's loaded variable-length transactions arrive one
+ * by one as a Poisson process of rate rate_tps; a host loop admits every
+ * arrived transaction (at most the admission cap) as the next batch once
+ * min_batch have arrived or the oldest has waited max_wait_us, runs it
+ * through the scheduler `s` (GCC_SCHED_LEARNED: predictor, deferral, probes
+ * and training; GCC_SCHED_PLAIN: plain ordering) and takes the time the
+ * batch's commit is visible on the host as the commit time of all its
+ * transactions. Table and CC state stay resident across batches (use
+ * GCC_F_NO_RESET to keep the metadata too). Schemes: tpl_nw, tpl_wd, silo,
+ * tictoc; warp_density 2..5. Synchronous; wall-clock paced. */
+typedef struct gcc_serve_params {
+    double rate_tps;        /* mean arrival rate, transactions / s */
+    uint64_t seed;          /* arrival process */
+    int32_t max_batch;      /* admission cap; 0 = what half the free device
+                               memory holds at the scheduler's footprint */
+    int32_t min_batch;      /* arrivals that start a batch at once (0 = 1) */
+    double max_wait_us;     /* ... or the oldest's wait (0 = 200 us) */
+} gcc_serve_params;
+
+typedef struct gcc_serve_result {
+    uint64_t committed, aborts, batches, admit_cap;
+    double offered_tps;      /* arrivals / s of the generated process */
+    double tx_per_s;         /* commits / s of wall time */
+    double device_tx_per_s;  /* commits / s of device time (the batches) */
+    double lat_p50_us, lat_p99_us, lat_max_us; /* arrival -> commit */
+    double mean_batch;       /* transactions per batch */
+    double busy_frac;        /* share of wall time spent in batches */
+    double sched_abort_rate; /* aborts / (aborts + commits) outside probes */
+} gcc_serve_result;
+
+int gcc_serve(gcc_sched *s, const gcc_run_params *rp, const gcc_serve_params *sp,
+              gcc_serve_result *out);
 
 #ifdef __cplusplus
 }

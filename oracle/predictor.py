@@ -123,3 +123,33 @@ def loss_and_grad(w: np.ndarray, feat: np.ndarray, y: np.ndarray, bf16: bool = T
     g[OFF_W1:OFF_B1] = (x.T @ dh1).ravel()
     g[OFF_B1:OFF_W2] = dh1.sum(axis=0)
     return loss, g
+
+
+def _var_keys(tx_off, reqs, lo, hi):
+    """Per-request (tx index, key, read word) of transactions lo .. hi-1."""
+    a, b = int(tx_off[lo]), int(tx_off[hi])
+    cnt = np.diff(tx_off[lo:hi + 1]).astype(np.int64)
+    tx = np.repeat(np.arange(hi - lo), cnt)
+    return tx, reqs["key"][a:b].astype(np.uint64), reqs["read"][a:b]
+
+
+def observe_var(freq: np.ndarray, tx_off, reqs, lo, hi) -> np.ndarray:
+    """observe() for variable-length transactions lo .. hi-1 (CSR)."""
+    _, keys, _ = _var_keys(tx_off, reqs, lo, hi)
+    f = freq >> np.uint32(1)
+    np.add.at(f, freq_slots(keys), np.uint32(1))
+    return f
+
+
+def features_var(tx_off, reqs, lo, hi, freq: np.ndarray) -> np.ndarray:
+    """features() for variable-length transactions lo .. hi-1: every request
+    counts (writes are requests whose read word is <= 0)."""
+    tx, keys, reads = _var_keys(tx_off, reqs, lo, hi)
+    out = np.zeros((hi - lo, FEAT_STRIDE), dtype=np.uint16)
+    bins = (splitmix64(keys) & np.uint64(63)).astype(np.int64)
+    np.add.at(out, (tx, bins), 1)
+    np.add.at(out[:, 64], tx, (reads <= 0).astype(np.uint16))
+    c = freq[freq_slots(keys)].astype(np.uint64) + np.uint64(1)
+    heat = np.floor(np.log2(c.astype(np.float64))).astype(np.uint16)
+    np.add.at(out[:, 65], tx, heat)
+    return out

@@ -115,7 +115,7 @@ def test_scheduled_runs_are_serializable(oracle, scheme, arm):
     with g.Engine(rows, layout=g.LAYOUT_U64X11, index=g.INDEX_HASH, fill_seed=8,
                   max_batch=4096) as eng, \
             g.Scheduler(eng, explore_every=3, probe_rows=512, train_steps=4 if arm == 0 else -1,
-                        minibatch=512, fixed_arm=arm) as sc:
+                        minibatch=512, fixed_arm=arm, defer_threshold=0.5) as sc:
         eng.load_txs(txs)
         if arm:
             sc.set_weights(_write_count_network())
