@@ -185,6 +185,7 @@ def library() -> C.CDLL:
         "gcc_destroy": (None, [P]),
         "gcc_load_txs": (C.c_int, [P, P, C.c_uint64]),
         "gcc_run": (C.c_int, [P, C.POINTER(RunParams), C.POINTER(Result)]),
+        "gcc_run_host": (C.c_int, [P, C.POINTER(RunParams), P, C.c_uint64, P, C.POINTER(Result)]),
         "gcc_run_checked": (C.c_int, [P, C.POINTER(RunParams), C.POINTER(Result),
                                       C.POINTER(C.c_int)]),
         "gcc_format_line": (C.c_int, [C.POINTER(RunParams), C.POINTER(Result), C.c_char_p,
@@ -355,6 +356,19 @@ class Engine:
         _check(self.lib.gcc_format_line(C.byref(p), C.byref(r), buf, 512), "gcc_format_line")
         out["line"] = buf.value.decode()
         return out
+
+    def run_host(self, scheme: str, txs: np.ndarray, digests: np.ndarray | None = None, **kw) -> dict:
+        """Run records that live in host memory (pinned for overlap): copies
+        in, batches and digest copies out overlap (gcc_run_host)."""
+        txs = np.ascontiguousarray(txs, dtype=TX_DTYPE)
+        p = self.params(scheme, **kw)
+        r = Result()
+        dp = None if digests is None else _ptr(digests)
+        rc = self.lib.gcc_run_host(self._h, C.byref(p), _ptr(txs), len(txs), dp, C.byref(r))
+        self.last_result = r.as_dict()
+        self.n_tx = len(txs)
+        _check(rc, f"gcc_run_host({scheme}) err_site={r.err_site}")
+        return r.as_dict()
 
     def run_checked(self, scheme: str, **kw) -> tuple[dict, bool]:
         """Run, then re-execute the committed transactions in their recorded

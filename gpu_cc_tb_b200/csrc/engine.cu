@@ -107,6 +107,9 @@ struct gcc_engine {
     int sm_count = 0;
     int clock_khz = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_in = nullptr, copy_out = nullptr;  // gcc_run_host transfers
+    const gcc_ycsb_tx *host_src = nullptr;              // set during gcc_run_host
+    uint64_t *host_dg = nullptr;
     cudaError_t last_cuda = cudaSuccess;
     gcc_table_desc desc{};
     uint32_t row_bytes = 0, stride = 0, words = 0, wslot = 0;
@@ -220,6 +223,8 @@ gcc_engine::~gcc_engine() {
         if (t) cudaFree(t);
     for (cudaEvent_t ev : events) cudaEventDestroy(ev);
     if (graph) cudaGraphExecDestroy(graph);
+    if (copy_in) cudaStreamDestroy(copy_in);
+    if (copy_out) cudaStreamDestroy(copy_out);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -501,6 +506,27 @@ int gcc_create(const gcc_table_desc *d, gcc_engine **out) {
 
 void gcc_destroy(gcc_engine *e) { delete e; }
 
+}  // extern "C"
+
+// Device buffers for n_tx 16-request records and their per-tx outputs.
+static int reserve_records(gcc_engine *e, uint64_t n_tx) {
+    int rc;
+    if (e->cap_rec < n_tx) {
+        if ((rc = e->alloc(&e->txs, n_tx * sizeof(gcc_ycsb_tx)))) return rc;
+        e->cap_rec = n_tx;
+    }
+    if (e->cap_tx < n_tx) {
+        if ((rc = e->alloc(&e->digest, n_tx * 8))) return rc;
+        if ((rc = e->alloc(&e->commit_hi, n_tx * 8))) return rc;
+        if ((rc = e->alloc(&e->commit_lo, n_tx * 8))) return rc;
+        if ((rc = e->alloc(&e->tx_aborts, n_tx * 4))) return rc;
+        e->cap_tx = n_tx;
+    }
+    return GCC_OK;
+}
+
+extern "C" {
+
 int gcc_load_txs(gcc_engine *e, const gcc_ycsb_tx *txs, uint64_t n_tx) {
     cudaGetLastError();  // a stale error of an earlier call is not ours
     if (!e || (!txs && n_tx)) return GCC_EINVAL;
@@ -612,7 +638,9 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
     p.ver_prev = e->ver_prev;
     p.ver_data = e->ver_data;
 
-    if ((rc = e->ensure_events(3 * nbatches + 4))) return rc;
+    const bool streamed = e->host_src != nullptr;
+    const uint64_t ev_copy = 3 * nbatches + 4;  // then nbatches copy-in, nbatches kernel-done
+    if ((rc = e->ensure_events(3 * nbatches + 4 + (streamed ? 2 * nbatches : 0)))) return rc;
     cudaEvent_t ev_start = e->events[0], ev_pre0 = e->events[1], ev_stop = e->events[2];
     const uint64_t launches0 = e->kernel_launches;
 
@@ -625,8 +653,22 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
     } while (0)
     CKR(cudaMemsetAsync(e->ctr, 0, sizeof(Counters), st));
     CKR(cudaEventRecord(ev_start, st));
+    if (streamed) {
+        // host records stream in batch by batch on their own stream; each
+        // batch waits only for its own records (gcc_run_host)
+        if (!e->copy_in) CKR(cudaStreamCreateWithFlags(&e->copy_in, cudaStreamNonBlocking));
+        if (!e->copy_out) CKR(cudaStreamCreateWithFlags(&e->copy_out, cudaStreamNonBlocking));
+        CKR(cudaStreamWaitEvent(e->copy_in, ev_start, 0));
+        for (uint64_t b = 0; b < nbatches; ++b) {
+            const uint64_t bst = b * batch, bn = std::min<uint64_t>(batch, e->n_tx - bst);
+            CKR(cudaMemcpyAsync(e->txs + bst, e->host_src + bst, bn * sizeof(gcc_ycsb_tx),
+                                cudaMemcpyHostToDevice, e->copy_in));
+            CKR(cudaEventRecord(e->events[ev_copy + b], e->copy_in));
+        }
+    }
     // GPUTx ranks every transaction once, before the batches (Init0).
     if (gputx) {
+        if (streamed) CKR(cudaStreamWaitEvent(st, e->events[ev_copy + nbatches - 1], 0));
         if ((rc = e->gputx_rank(p))) return rc;
         p.order = e->order;
     }
@@ -638,6 +680,7 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
         p.batch_st = (uint32_t)bst;
         p.batch_n = (uint32_t)bn;
         CKR(cudaEventRecord(e0, st));
+        if (streamed) CKR(cudaStreamWaitEvent(st, e->events[ev_copy + b], 0));
         // per-batch metadata reset (the reference memsets the whole table)
         const bool keep = (rp->flags & GCC_F_NO_RESET) &&
                           (s == S_TPL_NW || s == S_TPL_WD || s == S_SILO || s == S_TICTOC ||
@@ -664,9 +707,19 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
         CKR(launch_scheme_kernel(s, G, grid, block, p, st));
         e->kernel_launches += 1;
         CKR(cudaEventRecord(e2, st));
+        if (streamed && e->host_dg) {
+            // the batch's read digests go back while later batches run
+            CKR(cudaStreamWaitEvent(e->copy_out, e2, 0));
+            CKR(cudaMemcpyAsync(e->host_dg + bst, e->digest + bst, bn * 8, cudaMemcpyDeviceToHost,
+                                e->copy_out));
+        }
     }
     CKR(cudaEventRecord(ev_stop, st));
     CKR(cudaStreamSynchronize(st));
+    if (streamed) {
+        CKR(cudaStreamSynchronize(e->copy_in));
+        CKR(cudaStreamSynchronize(e->copy_out));
+    }
 #undef CKR
 
     Counters hc;
@@ -1112,6 +1165,25 @@ int gcc_get_batch_stats(gcc_engine *e, int32_t *wd, int32_t *bs, double *kms, ui
         kms[i] = e->bstat_ms[i];
     }
     return GCC_OK;
+}
+
+int gcc_run_host(gcc_engine *e, const gcc_run_params *rp, const gcc_ycsb_tx *host_txs,
+                 uint64_t n_tx, uint64_t *host_digests, gcc_result *out) {
+    cudaGetLastError();
+    if (!e || !rp || !host_txs || !out || n_tx == 0) return GCC_EINVAL;
+    if (n_tx >= (1ull << 27)) return GCC_EINVAL;
+    cudaSetDevice(e->dev);
+    int rc = reserve_records(e, n_tx);
+    if (rc) return rc;
+    e->n_tx = n_tx;
+    e->n_rec = n_tx;
+    e->have_run = false;
+    e->host_src = host_txs;
+    e->host_dg = host_digests;
+    rc = gcc_run(e, rp, out);
+    e->host_src = nullptr;
+    e->host_dg = nullptr;
+    return rc;
 }
 
 int gcc_run_checked(gcc_engine *e, const gcc_run_params *rp, gcc_result *out, int *verdict) {

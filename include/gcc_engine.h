@@ -362,6 +362,16 @@ int gcc_run_tpl_nw_noalloc(const gcc_ycsb_tx *txs, uint64_t n_tx, void *table,
                            uint64_t write_seed, void *stream, uint64_t *committed,
                            uint64_t *aborts);
 
+/* gcc_run with the records coming from host memory: batch b's records are
+ * copied on a copy stream while earlier batches execute, each batch waits
+ * only for its own records, and (if host_digests is not null) each batch's
+ * read digests are copied back while later batches execute. Results equal
+ * gcc_load_txs + gcc_run + gcc_get_digests; use pinned host memory for the
+ * copies to overlap. No counterpart in the reference (it reads the whole
+ * dataset first, benchmark_cpu/ycsb.cu:120-124). */
+int gcc_run_host(gcc_engine *e, const gcc_run_params *p, const gcc_ycsb_tx *host_txs,
+                 uint64_t n_tx, uint64_t *host_digests, gcc_result *out);
+
 /* Device-side timing of the last run's main kernels: total ms and number of
  * launches of the transaction kernel (for roofline accounting). */
 int gcc_last_kernel_ms(gcc_engine *e, double *kernel_ms, uint64_t *launches);
