@@ -76,7 +76,9 @@ def parse():
     ap.add_argument("--no-reset", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--sweep", default="", help="comma list of extra schemes to time once")
+    ap.add_argument("--sweep", default="tpl_wd,to,mvcc,silo,tictoc,gacco,gputx",
+                    help="comma list of extra schemes timed once on the same workload "
+                         "('' for none)")
     ap.add_argument("--workload", default="plain",
                     choices=["plain", "batched", "learned", "serving"],
                     help="plain: 1,048,576 x 16-request transactions in 65,536 batches; "
@@ -689,8 +691,10 @@ def main():
         if a.sweep:
             sw = {}
             for s in a.sweep.split(","):
+                eng.run(s, **kw)          # first run sizes the scheme's buffers
                 r = eng.run(s, **kw)
-                sw[s] = {"tx_per_s": r["tx_per_s"], "aborts": r["aborts"]}
+                sw[s] = {"tx_per_s": r["tx_per_s"], "aborts": r["aborts"],
+                         "p99_us": r["lat_p99_us"]}
             line["sweep"] = sw
         print(json.dumps(line), flush=True)
     eng.close()

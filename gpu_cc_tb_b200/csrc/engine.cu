@@ -681,11 +681,15 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
         p.batch_n = (uint32_t)bn;
         CKR(cudaEventRecord(e0, st));
         if (streamed) CKR(cudaStreamWaitEvent(st, e->events[ev_copy + b], 0));
-        // per-batch metadata reset (the reference memsets the whole table)
-        const bool keep = (rp->flags & GCC_F_NO_RESET) &&
-                          (s == S_TPL_NW || s == S_TPL_WD || s == S_SILO || s == S_TICTOC ||
-                           s == S_SLOW_TPL_NW || s == S_SLOW_TPL_WD || s == S_SLOW_SILO ||
-                           s == S_SLOW_TICTOC);
+        // per-batch metadata reset (the reference memsets the whole table).
+        // 2PL lock words are all zero again once a batch has committed every
+        // transaction (each lock taken is released), so for 2PL the memset
+        // of later batches would rewrite zeros with zeros and is skipped:
+        // the state is the reset state either way.
+        const bool tpl2 = s == S_TPL_NW || s == S_TPL_WD || s == S_SLOW_TPL_NW || s == S_SLOW_TPL_WD;
+        const bool keep = tpl2 || ((rp->flags & GCC_F_NO_RESET) &&
+                                   (s == S_SILO || s == S_TICTOC || s == S_SLOW_SILO ||
+                                    s == S_SLOW_TICTOC));
         if (!ordered && !(keep && b > 0)) CKR(cudaMemsetAsync(e->meta, 0, e->rows * 8, st));
         if (is_mvcc(s)) CKR(cudaMemsetAsync(e->turn, 0xFF, e->rows * 4, st));
         k_batch_prep<<<1, 32, 0, st>>>(e->ctr, uses_ts(s) ? 1 : 0);
