@@ -14,6 +14,12 @@
 //   write=rowcopy|field    write semantics (default rowcopy)
 //   fill_seed=N            row fields from seed N (default 0: zero fields)
 //   device=N  spin_ms=N  backoff_ns=N
+// Result files (headerless little-endian arrays, for parity tooling):
+//   table_out=PATH       final rows, packed (104 or 88 bytes each)
+//   digests_out=PATH     u64 read digest per transaction
+//   commit_log_out=PATH  {u64 hi, u64 lo} serialization key per transaction
+//   aborts_out=PATH      u32 aborted attempts per transaction
+//   read_log_out=PATH    every read row image, txcnt x 16 slots of 112 / 96 B
 // debug_flag=1 additionally re-executes the committed transactions in their
 // recorded serialization order on the GPU and compares final table and read
 // digests: prints GOOD or BAD (the reference's debug check prints GOOD/BAD
@@ -65,6 +71,7 @@ int main(int argc, char **argv) {
     rp.batch_size = batch;
     rp.write_mode = GCC_WRITE_ROWCOPY;
     rp.write_seed = 1;
+    std::string table_out, digests_out, commit_out, aborts_out, readlog_out;
     for (int i = 9; i < argc; ++i) {
         std::string kv(argv[i]);
         size_t eq = kv.find('=');
@@ -77,7 +84,14 @@ int main(int argc, char **argv) {
         else if (k == "device") desc.device = std::atoi(v.c_str());
         else if (k == "spin_ms") rp.spin_limit_ns = std::strtoull(v.c_str(), nullptr, 10) * 1000000ull;
         else if (k == "backoff_ns") rp.backoff_ns = std::atoi(v.c_str());
+        else if (k == "table_out") table_out = v;
+        else if (k == "digests_out") digests_out = v;
+        else if (k == "commit_log_out") commit_out = v;
+        else if (k == "aborts_out") aborts_out = v;
+        else if (k == "read_log_out") readlog_out = v;
     }
+    if (!commit_out.empty()) rp.flags |= GCC_F_COMMIT_LOG;
+    if (!readlog_out.empty()) rp.flags |= GCC_F_READ_LOG;
     std::cout << "TRY " << argv[4] << "," << wd << "," << bs << "," << batch << "\n";
 
     std::vector<gcc_ycsb_tx> txs((size_t)txcnt);
@@ -123,6 +137,41 @@ int main(int argc, char **argv) {
               << "proc " << (float)r.proc_s << ",\n"
               << "tot " << (float)r.tot_s << "\n";
     if (debug) std::cout << (verdict == 1 ? "GOOD" : "BAD") << "\n";
+    // result files
+    auto write_file = [&](const std::string &path, const void *data, size_t bytes) -> bool {
+        FILE *o = std::fopen(path.c_str(), "wb");
+        if (!o) { std::perror(path.c_str()); return false; }
+        const bool ok = std::fwrite(data, 1, bytes, o) == bytes;
+        std::fclose(o);
+        return ok;
+    };
+    const uint64_t n = (uint64_t)txcnt;
+    bool files_ok = true;
+    if (!table_out.empty()) {
+        std::vector<uint8_t> t((size_t)rownum * gcc_row_bytes(desc.layout));
+        if ((rc = gcc_dump_table(e, t.data(), t.size()))) { gcc_destroy(e); return die("gcc_dump_table", rc); }
+        files_ok &= write_file(table_out, t.data(), t.size());
+    }
+    if (!digests_out.empty()) {
+        std::vector<uint64_t> d(n);
+        if ((rc = gcc_get_digests(e, d.data(), n))) { gcc_destroy(e); return die("gcc_get_digests", rc); }
+        files_ok &= write_file(digests_out, d.data(), d.size() * 8);
+    }
+    if (!commit_out.empty()) {
+        std::vector<gcc_commit_rec> c(n);
+        if ((rc = gcc_get_commit_log(e, c.data(), n))) { gcc_destroy(e); return die("gcc_get_commit_log", rc); }
+        files_ok &= write_file(commit_out, c.data(), c.size() * sizeof(gcc_commit_rec));
+    }
+    if (!aborts_out.empty()) {
+        std::vector<uint32_t> a(n);
+        if ((rc = gcc_get_tx_aborts(e, a.data(), n))) { gcc_destroy(e); return die("gcc_get_tx_aborts", rc); }
+        files_ok &= write_file(aborts_out, a.data(), a.size() * 4);
+    }
+    if (!readlog_out.empty()) {
+        std::vector<uint8_t> l((size_t)n * 16 * gcc_row_stride(desc.layout));
+        if ((rc = gcc_get_read_log(e, l.data(), l.size()))) { gcc_destroy(e); return die("gcc_get_read_log", rc); }
+        files_ok &= write_file(readlog_out, l.data(), l.size());
+    }
     gcc_destroy(e);
-    return 0;
+    return files_ok ? 0 : 1;
 }

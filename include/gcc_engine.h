@@ -334,7 +334,8 @@ int gcc_upload_table(gcc_engine *e, const void *host_src, uint64_t bytes);
 int gcc_get_digests(gcc_engine *e, uint64_t *dst, uint64_t n_tx);
 int gcc_get_commit_log(gcc_engine *e, gcc_commit_rec *dst, uint64_t n_tx);
 int gcc_get_tx_aborts(gcc_engine *e, uint32_t *dst, uint64_t n_tx);
-/* Read log: n_tx * 16 row images of row_bytes each (slot = tx*16 + op). */
+/* Read log: n_tx * 16 slots of gcc_row_stride(layout) bytes (slot = tx*16 +
+ * op), each holding the row image that read request read (row_bytes used). */
 int gcc_get_read_log(gcc_engine *e, void *dst, uint64_t bytes);
 /* Index probe for n keys (testing the index): rows[i] = row or UINT32_MAX. */
 int gcc_index_lookup(gcc_engine *e, const uint32_t *keys, uint32_t *rows,

@@ -61,3 +61,35 @@ def test_run_checked_api():
                                           write_mode=mode)
                 assert ok, (scheme, mode)
                 assert res["committed"] == len(txs)
+
+
+@pytest.mark.parametrize("scheme", ["tpl_nw", "tictoc", "gacco"])
+def test_test_ycsb_result_files(oracle, dataset, scheme, tmp_path):
+    # the reference's setup (104-byte rows, sorted index, whole-row copies)
+    # with every result file written; the files reproduce the oracle's
+    # serial replay in the logged order
+    outs = {k: tmp_path / f"{k}.bin" for k in ("table", "digests", "commit_log", "aborts", "read_log")}
+    args = [str(BIN / "test_ycsb"), str(dataset), "4096", "8192", scheme, "5", "8", "2048", "0"]
+    args += [f"{k}_out={v}" for k, v in outs.items()]
+    out = subprocess.run(args, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    txs = np.frombuffer(dataset.read_bytes(), dtype=g.TX_DTYPE)
+    layout = g.LAYOUT_REF104
+    table = np.frombuffer(outs["table"].read_bytes(), dtype=np.uint8).reshape(4096, 104)
+    dg = np.frombuffer(outs["digests"].read_bytes(), dtype=np.uint64)
+    log = np.frombuffer(outs["commit_log"].read_bytes(), dtype=np.uint64).reshape(-1, 2)
+    aborts = np.frombuffer(outs["aborts"].read_bytes(), dtype=np.uint32)
+    rl = np.frombuffer(outs["read_log"].read_bytes(), dtype=np.uint8).reshape(8192, 16, 112)
+    assert len(dg) == len(log) == len(aborts) == 8192
+    order = np.arange(8192) if scheme == "gacco" else oracle.commit_order(log)
+    init = oracle.fill_table(4096, layout, 0)
+    ref_t, ref_dg, ref_rl = oracle.replay(init, layout, txs, order, g.WRITE_ROWCOPY, 1,
+                                          read_log=True)
+    assert np.array_equal(table, ref_t)
+    assert np.array_equal(dg, ref_dg)
+    for t in range(0, 8192, 97):
+        for i in range(int(txs[t]["request_cnt"])):
+            if txs[t]["requests"][i]["read"]:
+                assert np.array_equal(rl[t, i, :104], ref_rl[t, i, :104]), (t, i)
+    if scheme == "gacco":
+        assert not aborts.any()
