@@ -521,8 +521,10 @@ def run_serving(a):
     clocks.start()
     peak = {"on": [], "off": []}
     dev = {"on": [], "off": []}
+    launches = 0
     for _ in range(a.steps):
         r = on.serve(sch, rate_tps=1e10, seed=2, max_batch=65536, **kw)
+        launches += r["kernel_launches"]
         peak["on"].append(r["tx_per_s"])
         dev["on"].append(r["device_tx_per_s"])
         r = off_s.serve(sch, rate_tps=1e10, seed=2, max_batch=65536, **kw)
@@ -573,7 +575,7 @@ def run_serving(a):
             "e2e": {"value": job["e2e_value"], "unit": "tx/s",
                     "h2d_bytes_per_step": int(reqs[:int(off[n_peak])].nbytes + 4 * (n_peak + 1)),
                     "d2h_bytes_per_step": 0},
-            "gpu_launches": None,
+            "gpu_launches": int(launches // a.steps),
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)

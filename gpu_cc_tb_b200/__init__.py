@@ -151,7 +151,8 @@ class ServeResult(C.Structure):
                 ("admit_cap", C.c_uint64), ("offered_tps", C.c_double), ("tx_per_s", C.c_double),
                 ("device_tx_per_s", C.c_double), ("lat_p50_us", C.c_double),
                 ("lat_p99_us", C.c_double), ("lat_max_us", C.c_double), ("mean_batch", C.c_double),
-                ("busy_frac", C.c_double), ("sched_abort_rate", C.c_double)]
+                ("busy_frac", C.c_double), ("sched_abort_rate", C.c_double),
+                ("kernel_launches", C.c_uint64)]
 
 
 SCHED_PLAIN, SCHED_LEARNED = 0, 1

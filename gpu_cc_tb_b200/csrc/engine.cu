@@ -2209,6 +2209,7 @@ int gcc_serve(gcc_sched *sc, const gcc_run_params *rp, const gcc_serve_params *s
     out->mean_batch = out->batches ? (double)n / (double)out->batches : 0.0;
     out->busy_frac = wall > 0 ? busy / wall : 0.0;
     out->sched_abort_rate = sr.sched_abort_rate;
+    out->kernel_launches = sr.run.kernel_launches;
     return GCC_OK;
 }
 

@@ -517,6 +517,7 @@ typedef struct gcc_serve_result {
     double mean_batch;       /* transactions per batch */
     double busy_frac;        /* share of wall time spent in batches */
     double sched_abort_rate; /* aborts / (aborts + commits) outside probes */
+    uint64_t kernel_launches;/* engine kernels launched by the run */
 } gcc_serve_result;
 
 int gcc_serve(gcc_sched *s, const gcc_run_params *rp, const gcc_serve_params *sp,
