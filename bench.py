@@ -46,6 +46,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -124,8 +125,8 @@ class Clocks:
         self.dev, self.proc, self.path = dev, None, None
 
     def start(self):
-        out = ROOT / "gpurun_out"
-        out.mkdir(exist_ok=True)
+        out = Path(os.environ.get("BENCH_CLOCKS_DIR", tempfile.gettempdir()))
+        out.mkdir(parents=True, exist_ok=True)
         self.path = out / f"clocks_{os.getpid()}.csv"
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
