@@ -691,6 +691,26 @@ def main():
         if not a.no_cpu_baseline and ws == 1:
             from oracle import oracle_py as o
             line["cpu_baseline"], _ = cpu_baseline(g, o, txs, a, a.cpu_threads)
+        if ws == 1:
+            # the reference's CPU-runnable shape (1,048,576 rows, 65,536
+            # transactions, theta 0.1, one batch): the same kernel at low
+            # contention, for the roofline
+            c0 = g.gen_ycsb(1_048_576, 65_536, 0.1, a.read_ratio, seed=141919810,
+                            dedup=g.DEDUP_RESAMPLE, key_base=0)
+            b0, _, _ = algorithmic_bytes(c0)
+            with g.Engine(1_048_576, layout=g.LAYOUT_U64X11, index=index, fill_seed=141919810,
+                          device=local, max_batch=65_536) as e0:
+                e0.load_txs(c0)
+                k0 = dict(kw, batch_size=65_536)
+                for _ in range(3):
+                    e0.run(a.scheme, **k0)
+                rs = [e0.run(a.scheme, **k0) for _ in range(5)]
+                kms = e0.last_kernel_ms()[0]
+            ach = b0 / (kms / 1000) / 1e9
+            line["config0"] = {"workload": "ycsb_plain_1048576rows_65536tx_16ops_theta0.1_r0.9",
+                               "tx_per_s": statistics.median(r["tx_per_s"] for r in rs),
+                               "kernel_ms": kms, "achieved_gbs": ach, "frac_of_hbm": ach / hbm,
+                               "note": "one launch of 65,536 transactions at low contention"}
         if a.sweep:
             sw = {}
             for s in a.sweep.split(","):

@@ -51,6 +51,27 @@ uint64_t active_grid(int32_t max_active, int G, int block) {
     return std::max<uint64_t>(1, ((uint64_t)max_active * G + block - 1) / block);
 }
 
+// Latency percentile q (0..1) of a run's log-linear histogram in
+// microseconds: the upper edge of the bucket that reaches the q-th
+// transaction (buckets: 1 ns below 16 ns, then 16 linear steps per octave).
+double hist_percentile_us(const Counters &hc, double q) {
+    uint64_t total = 0;
+    for (int i = 0; i < kHistBuckets; ++i) total += hc.hist[i];
+    if (!total) return 0.0;
+    auto edge = [](int b) -> double {
+        if (b < 16) return (double)b + 1.0;
+        const int lg = b / 16 + 3, sub = b % 16;
+        return std::ldexp(16.0 + sub + 1.0, lg - 4);
+    };
+    const uint64_t target = (uint64_t)std::ceil(q * (double)total);
+    uint64_t acc = 0;
+    for (int i = 0; i < kHistBuckets; ++i) {
+        acc += hc.hist[i];
+        if (acc >= target) return edge(i) / 1000.0;
+    }
+    return edge(kHistBuckets - 1) / 1000.0;
+}
+
 // starve_limit of gcc_run_params -> kernel value (0: off)
 uint32_t starve_param(int32_t v) { return v < 0 ? 0u : (v == 0 ? 32u : (uint32_t)v); }
 
@@ -764,24 +785,8 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
     out->max_attempts = hc.max_attempts;
     out->err_site = hc.err_where;
     // latency percentiles from the histogram (bucket upper edges)
-    uint64_t total = 0;
-    for (int i = 0; i < kHistBuckets; ++i) total += hc.hist[i];
-    auto edge = [](int b) -> double {
-        if (b < 16) return (double)b + 1.0;
-        int lg = b / 16 + 3, sub = b % 16;
-        return std::ldexp(16.0 + sub + 1.0, lg - 4);
-    };
-    auto pct = [&](double q) -> double {
-        if (!total) return 0.0;
-        uint64_t target = (uint64_t)std::ceil(q * (double)total), acc = 0;
-        for (int i = 0; i < kHistBuckets; ++i) {
-            acc += hc.hist[i];
-            if (acc >= target) return edge(i) / 1000.0;
-        }
-        return edge(kHistBuckets - 1) / 1000.0;
-    };
-    out->lat_p50_us = pct(0.50);
-    out->lat_p99_us = pct(0.99);
+    out->lat_p50_us = hist_percentile_us(hc, 0.50);
+    out->lat_p99_us = hist_percentile_us(hc, 0.99);
     if (hc.err) return (int)hc.err;
     if (hc.committed != e->n_tx) return GCC_ESTATE;
     return GCC_OK;
@@ -1130,24 +1135,8 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
     out->kernel_launches = mode == GCC_BATCHES_QUEUE ? 3 : 2 * nb;
     out->max_attempts = hc.max_attempts;
     out->err_site = hc.err_where;
-    uint64_t total = 0;
-    for (int i = 0; i < kHistBuckets; ++i) total += hc.hist[i];
-    auto edge = [](int b) -> double {
-        if (b < 16) return (double)b + 1.0;
-        int lg = b / 16 + 3, sub = b % 16;
-        return std::ldexp(16.0 + sub + 1.0, lg - 4);
-    };
-    auto pct = [&](double q) -> double {
-        if (!total) return 0.0;
-        uint64_t target = (uint64_t)std::ceil(q * (double)total), acc = 0;
-        for (int i = 0; i < kHistBuckets; ++i) {
-            acc += hc.hist[i];
-            if (acc >= target) return edge(i) / 1000.0;
-        }
-        return edge(kHistBuckets - 1) / 1000.0;
-    };
-    out->lat_p50_us = pct(0.50);
-    out->lat_p99_us = pct(0.99);
+    out->lat_p50_us = hist_percentile_us(hc, 0.50);
+    out->lat_p99_us = hist_percentile_us(hc, 0.99);
     if (hc.err) return (int)hc.err;
     if (hc.committed != e->n_var) return GCC_ESTATE;
     return GCC_OK;
@@ -2059,24 +2048,8 @@ int sched_finish(SchedRun &R, uint64_t n, uint64_t nb, gcc_sched_result *out) {
     r->kernel_launches = e->kernel_launches - R.launches0;
     r->max_attempts = hc.max_attempts;
     r->err_site = hc.err_where;
-    uint64_t total = 0;
-    for (int i = 0; i < kHistBuckets; ++i) total += hc.hist[i];
-    auto edge = [](int bk) -> double {
-        if (bk < 16) return (double)bk + 1.0;
-        int lg = bk / 16 + 3, sub = bk % 16;
-        return std::ldexp(16.0 + sub + 1.0, lg - 4);
-    };
-    auto pct = [&](double q) -> double {
-        if (!total) return 0.0;
-        uint64_t target = (uint64_t)std::ceil(q * (double)total), acc = 0;
-        for (int i = 0; i < kHistBuckets; ++i) {
-            acc += hc.hist[i];
-            if (acc >= target) return edge(i) / 1000.0;
-        }
-        return edge(kHistBuckets - 1) / 1000.0;
-    };
-    r->lat_p50_us = pct(0.50);
-    r->lat_p99_us = pct(0.99);
+    r->lat_p50_us = hist_percentile_us(hc, 0.50);
+    r->lat_p99_us = hist_percentile_us(hc, 0.99);
     for (auto &rec : sc->batches) {
         out->probed += rec.probe;
         out->deferred += rec.deferred;
