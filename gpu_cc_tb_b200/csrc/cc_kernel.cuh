@@ -1163,14 +1163,18 @@ GCC_D int attempt(const KParams &p, const Group<G> &g, const TX &s, uint32_t tx,
 __host__ __device__ constexpr bool is_ordered(int s) { return s == S_GACCO || s == S_GPUTX; }
 
 // Attempts before retries switch to one request at a time in key order.
-// The first 3 retries of TO, 2PL, Silo and TicToc take their requests in
-// parallel like the first attempt; only later ones go one request at a time
-// in key order. The starvation control bounds the cycles that made fully
-// parallel retries livelock. Measured at theta 0.6: TO 22.9 -> 32.1, tpl_nw
-// 59.7 -> 65.7, silo 147 -> 168, tictoc 147 -> 165 M tx/s; within noise at
-// theta 0.99. The latch variants go ordered from the first retry.
+// Retries take their requests in parallel like the first attempt: Silo and
+// TicToc always, TO and 2PL for their first 15 retries, after which they go
+// one request at a time in key order. The starvation control bounds the
+// cycles that made fully parallel retries livelock. Measured (10,485,760
+// rows, r 0.9) against ordering from the first retry: silo / tictoc +40 %
+// at theta 0.6 and +25-50 % at 0.8-0.99; TO 22.9 -> 57 M tx/s at 0.6 and
+// unchanged at 0.8-0.99; tpl_nw 58 -> 67 M at 0.6, -5 % at 0.8, unchanged
+// at 0.9-0.99 (never ordering 2PL / TO gives 98 M at 0.6 but -35 % at 0.8
+// and above). The latch variants go ordered from the first retry.
 __host__ __device__ constexpr unsigned ordered_after(int s) {
-    return (s == S_TO || s == S_TPL_NW || s == S_TPL_WD || s == S_SILO || s == S_TICTOC) ? 4u : 1u;
+    return (s == S_SILO || s == S_TICTOC) ? 0xFFFFFFFFu
+                                          : ((s == S_TO || s == S_TPL_NW || s == S_TPL_WD) ? 16u : 1u);
 }
 
 // ===========================================================================
