@@ -491,6 +491,27 @@ def run_learned(a):
         dist.destroy_process_group()
 
 
+def serving_cpu_baseline(g, d, off, reqs, sch, a, n=200_000):
+    """The CPU executors (oracle port of the CC rules, all host threads) on
+    the first n order-entry transactions, closed loop (all arrived)."""
+    try:
+        from oracle import oracle_py as o
+        tx_off = np.ascontiguousarray(off[:n + 1])
+        rq = reqs[:int(off[n])]
+        lay_rows = int(rq["key"].max()) + 1
+        init = o.fill_table(lay_rows, g.LAYOUT_U64X11, 141919810)
+        kind = sch if sch in ("tpl_nw", "silo", "tictoc") else "tpl_nw"
+        threads = a.cpu_threads or os.cpu_count()
+        _, _, _, secs, aborts = o.cpu_run_var(kind, init, g.LAYOUT_U64X11, tx_off, rq,
+                                              g.WRITE_FIELD, 1, ext_ops=True, threads=threads,
+                                              commit_log=False)
+        return {"value": n / secs if secs > 0 else 0.0, "unit": "tx/s", "cores": threads,
+                "kind": "port", "scheme": kind, "aborts": int(aborts),
+                "sample": f"first {n} order-entry transactions, closed loop, {threads} threads"}
+    except Exception as ex:  # the GPU line stays valid without it
+        return {"error": str(ex)[:200]}
+
+
 def run_serving(a):
     """Order-entry serving: peak (saturated) commits/s and a Poisson load
     sweep with p50/p99 latency, learned scheduler on vs off."""
@@ -556,6 +577,7 @@ def run_serving(a):
         sweep.append(pt)
     job = replicas.combine(dist, n_peak * a.steps / p_on, n_peak * a.steps, e2e_s, a.steps * n_peak)
     if rank == 0:
+        cpu = serving_cpu_baseline(g, d, off, reqs, sch, a)
         line = {
             "metric": "committed tx/s (learned vs plain CC, same GPU, 0 violations); p99",
             "value": job["value"], "unit": "tx/s", "n_gpus": ws, "steps": a.steps,
@@ -577,6 +599,7 @@ def run_serving(a):
                     "h2d_bytes_per_step": int(reqs[:int(off[n_peak])].nbytes + 4 * (n_peak + 1)),
                     "d2h_bytes_per_step": 0},
             "gpu_launches": int(launches // a.steps),
+            "cpu_baseline": cpu,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)

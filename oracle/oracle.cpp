@@ -304,13 +304,24 @@ struct Cpu {
     uint32_t rb, words;
     int32_t write_mode;
     uint64_t wseed;
+    bool ext = false;  // negative read words are extended ops
     std::atomic<uint64_t> *meta;
     std::atomic<uint64_t> seq{0};
-    const gcc_ycsb_tx *txs;
+    // transactions: 16-request records, or CSR (tx_off, reqs)
+    const gcc_ycsb_tx *txs = nullptr;
+    const uint32_t *tx_off = nullptr;
+    const gcc_ycsb_req *reqs = nullptr;
     uint64_t n_tx;
     uint64_t *digests;
     gcc_commit_rec *log;
 
+    uint32_t n_req(uint32_t t) const {
+        return txs ? (uint32_t)txs[t].request_cnt : tx_off[t + 1] - tx_off[t];
+    }
+    const gcc_ycsb_req &req(uint32_t t, uint32_t i) const {
+        return txs ? txs[t].requests[i] : reqs[tx_off[t] + i];
+    }
+    bool is_read(uint32_t t, uint32_t i) const { return req(t, i).read > 0; }
     uint64_t *rowp(uint64_t r) const { return (uint64_t *)(table + r * rb); }
     uint64_t ld(const uint64_t *p) const { return __atomic_load_n(p, __ATOMIC_RELAXED); }
     void st(uint64_t *p, uint64_t v) const { __atomic_store_n(p, v, __ATOMIC_RELAXED); }
@@ -323,35 +334,70 @@ struct Cpu {
         }
         return d;
     }
-    void write_op(uint64_t r, uint32_t tx, uint32_t i, const uint64_t *item) const {
+    // Extended op on a row held exclusively (same rules as ext_op above,
+    // with the executors' atomic word accesses); returns its digest term.
+    uint64_t ext_write(uint64_t r, uint32_t tx, uint32_t i, uint32_t w) const {
         uint64_t *p = rowp(r);
+        const uint32_t op = (w >> 28) & 7u, f = (w >> 24) & 15u, v = w & 0xFFFFFFu;
+        if (op == GCC_OP_INSERT) {
+            st(p + 1, tx);
+            st(p + 2, v);
+            for (uint32_t k = 0; k < 8; ++k) st(p + 3 + k, h3(wseed, tx, 1024ull + i * 8ull + k));
+            return 0;
+        }
+        uint64_t dt = 0;
+        for (uint32_t k = 0; k < words; ++k) dt += term(ld(p + k), i, k);
+        uint64_t *fw = p + 1 + f;
+        const uint64_t a = ld(fw);
+        if (op == GCC_OP_ADD) st(fw, a + v);
+        else if (op == GCC_OP_SUB) st(fw, a - v);
+        else if (op == GCC_OP_STOCK) {
+            const uint64_t q = v & 0xFFu, remote = (v >> 8) & 1u;
+            st(fw, a >= q + 10 ? a - q : a - q + 91);
+            st(fw + 1, ld(fw + 1) + q);
+            st(fw + 2, ld(fw + 2) + 1);
+            st(fw + 3, ld(fw + 3) + remote);
+        } else if (op == GCC_OP_PAY) {
+            st(fw, a - v);
+            st(fw + 1, ld(fw + 1) + v);
+            st(fw + 2, ld(fw + 2) + 1);
+        }
+        return dt;
+    }
+    // write request i of tx (field write, row copy, or extended op)
+    uint64_t write_op(uint32_t tx, uint32_t i, const uint64_t *item) const {
+        const gcc_ycsb_req &rq = req(tx, i);
+        if (ext && rq.read < 0) return ext_write(rq.key, tx, i, (uint32_t)rq.read);
+        uint64_t *p = rowp(rq.key);
         if (write_mode == GCC_WRITE_FIELD) {
             uint32_t f = (uint32_t)(h3(wseed, tx, 2ull * i) % 10ull);
             st(p + 1 + f, h3(wseed, tx, 2ull * i + 1));
         } else {
             for (uint32_t k = 0; k < words; ++k) st(p + k, item[k]);
         }
+        return 0;
     }
 };
 
 constexpr uint64_t kExcl = 1ull << 31;
 constexpr uint64_t kLock = 1ull << 63;
+constexpr uint32_t kCpuMaxReq = 64;
 
 // Source image for a rowcopy write: the last read before op i.
-const uint64_t *src_image(const gcc_ycsb_tx &tx, uint32_t i, const std::vector<uint64_t> &imgs,
-                          uint32_t words, const std::vector<uint64_t> &zero) {
+const uint64_t *src_image(const Cpu &c, uint32_t t, uint32_t i, const std::vector<uint64_t> &imgs,
+                          const std::vector<uint64_t> &zero) {
     for (int j = (int)i - 1; j >= 0; --j)
-        if (tx.requests[j].read) return imgs.data() + (size_t)j * words;
+        if (c.is_read(t, (uint32_t)j)) return imgs.data() + (size_t)j * c.words;
     return zero.data();
 }
 
 bool tx_tpl_nw(Cpu &c, uint32_t t, std::vector<uint64_t> &imgs, const std::vector<uint64_t> &zero) {
-    const gcc_ycsb_tx &tx = c.txs[t];
-    uint32_t n = (uint32_t)tx.request_cnt, held = 0;
+    const uint32_t n = c.n_req(t);
+    uint32_t held = 0;
     for (uint32_t i = 0; i < n; ++i) {
-        std::atomic<uint64_t> &m = c.meta[tx.requests[i].key];
+        std::atomic<uint64_t> &m = c.meta[c.req(t, i).key];
         bool ok;
-        if (tx.requests[i].read) {
+        if (c.is_read(t, i)) {
             uint64_t old = m.fetch_add(1, std::memory_order_acq_rel);
             ok = !(old & kExcl);
             if (!ok) m.fetch_sub(1, std::memory_order_acq_rel);
@@ -361,8 +407,8 @@ bool tx_tpl_nw(Cpu &c, uint32_t t, std::vector<uint64_t> &imgs, const std::vecto
         }
         if (!ok) {
             for (uint32_t j = 0; j < held; ++j) {
-                std::atomic<uint64_t> &mj = c.meta[tx.requests[j].key];
-                if (tx.requests[j].read) mj.fetch_sub(1, std::memory_order_acq_rel);
+                std::atomic<uint64_t> &mj = c.meta[c.req(t, j).key];
+                if (c.is_read(t, j)) mj.fetch_sub(1, std::memory_order_acq_rel);
                 else mj.fetch_and(0x7FFFFFFFull, std::memory_order_acq_rel);
             }
             return false;
@@ -372,13 +418,12 @@ bool tx_tpl_nw(Cpu &c, uint32_t t, std::vector<uint64_t> &imgs, const std::vecto
     if (c.log) c.log[t] = gcc_commit_rec{c.seq.fetch_add(1), 0};
     uint64_t dg = 0;
     for (uint32_t i = 0; i < n; ++i)
-        if (tx.requests[i].read) dg += c.read_row(tx.requests[i].key, i, imgs.data() + (size_t)i * c.words);
+        if (c.is_read(t, i)) dg += c.read_row(c.req(t, i).key, i, imgs.data() + (size_t)i * c.words);
     for (uint32_t i = 0; i < n; ++i)
-        if (!tx.requests[i].read)
-            c.write_op(tx.requests[i].key, t, i, src_image(tx, i, imgs, c.words, zero));
+        if (!c.is_read(t, i)) dg += c.write_op(t, i, src_image(c, t, i, imgs, zero));
     for (uint32_t i = 0; i < n; ++i) {
-        std::atomic<uint64_t> &m = c.meta[tx.requests[i].key];
-        if (tx.requests[i].read) m.fetch_sub(1, std::memory_order_acq_rel);
+        std::atomic<uint64_t> &m = c.meta[c.req(t, i).key];
+        if (c.is_read(t, i)) m.fetch_sub(1, std::memory_order_acq_rel);
         else m.fetch_and(0x7FFFFFFFull, std::memory_order_acq_rel);
     }
     c.digests[t] = dg;
@@ -387,17 +432,16 @@ bool tx_tpl_nw(Cpu &c, uint32_t t, std::vector<uint64_t> &imgs, const std::vecto
 
 template <bool TICTOC>
 bool tx_occ(Cpu &c, uint32_t t, std::vector<uint64_t> &imgs, const std::vector<uint64_t> &zero) {
-    const gcc_ycsb_tx &tx = c.txs[t];
-    uint32_t n = (uint32_t)tx.request_cnt;
-    uint64_t rec[16], dg = 0;
+    const uint32_t n = c.n_req(t);
+    uint64_t rec[kCpuMaxReq], dg = 0;
     const uint64_t wmask = (1ull << 48) - 1;
     for (uint32_t i = 0; i < n; ++i) {
-        if (!tx.requests[i].read) continue;
-        std::atomic<uint64_t> &m = c.meta[tx.requests[i].key];
+        if (!c.is_read(t, i)) continue;
+        std::atomic<uint64_t> &m = c.meta[c.req(t, i).key];
         while (true) {
             uint64_t x1 = m.load(std::memory_order_acquire);
             if (x1 & kLock) continue;
-            uint64_t d = c.read_row(tx.requests[i].key, i, imgs.data() + (size_t)i * c.words);
+            uint64_t d = c.read_row(c.req(t, i).key, i, imgs.data() + (size_t)i * c.words);
             std::atomic_thread_fence(std::memory_order_acquire);
             if (m.load(std::memory_order_acquire) != x1) continue;
             rec[i] = x1;
@@ -405,19 +449,19 @@ bool tx_occ(Cpu &c, uint32_t t, std::vector<uint64_t> &imgs, const std::vector<u
             break;
         }
     }
-    uint32_t locked = 0;
+    uint64_t locked = 0;
     uint64_t cts = 0;
     bool fail = false;
     for (uint32_t i = 0; i < n && !fail; ++i) {
-        if (tx.requests[i].read) continue;
-        std::atomic<uint64_t> &m = c.meta[tx.requests[i].key];
+        if (c.is_read(t, i)) continue;
+        std::atomic<uint64_t> &m = c.meta[c.req(t, i).key];
         uint64_t x = m.load(std::memory_order_acquire);
         while (true) {
             if (x & kLock) { fail = true; break; }
             if (m.compare_exchange_weak(x, x | kLock, std::memory_order_acq_rel)) break;
         }
         if (fail) break;
-        locked |= 1u << i;
+        locked |= 1ull << i;
         uint64_t c1 = TICTOC ? (x & wmask) + ((x >> 48) & 0x7FFF) + 1 : (x & ~kLock);
         cts = std::max(cts, c1);
     }
@@ -426,20 +470,20 @@ bool tx_occ(Cpu &c, uint32_t t, std::vector<uint64_t> &imgs, const std::vector<u
     if (!fail) {
         if (!TICTOC) {
             for (uint32_t i = 0; i < n && !fail; ++i) {
-                if (!tx.requests[i].read) continue;
-                uint64_t x = c.meta[tx.requests[i].key].load(std::memory_order_acquire);
+                if (!c.is_read(t, i)) continue;
+                uint64_t x = c.meta[c.req(t, i).key].load(std::memory_order_acquire);
                 if (x != rec[i]) fail = true;  // ts changed or locked
                 cts = std::max(cts, rec[i] & ~kLock);
             }
             cts += 1;
         } else {
             for (uint32_t i = 0; i < n; ++i)
-                if (tx.requests[i].read) cts = std::max(cts, rec[i] & wmask);
+                if (c.is_read(t, i)) cts = std::max(cts, rec[i] & wmask);
             for (uint32_t i = 0; i < n && !fail; ++i) {
-                if (!tx.requests[i].read) continue;
+                if (!c.is_read(t, i)) continue;
                 uint64_t rwts = rec[i] & wmask, rrts = rwts + ((rec[i] >> 48) & 0x7FFF);
                 if (rrts >= cts) continue;
-                std::atomic<uint64_t> &m = c.meta[tx.requests[i].key];
+                std::atomic<uint64_t> &m = c.meta[c.req(t, i).key];
                 while (true) {
                     uint64_t x = m.load(std::memory_order_acquire);
                     uint64_t wts = x & wmask, rts = wts + ((x >> 48) & 0x7FFF);
@@ -455,53 +499,30 @@ bool tx_occ(Cpu &c, uint32_t t, std::vector<uint64_t> &imgs, const std::vector<u
     }
     if (fail) {
         for (uint32_t i = 0; i < n; ++i)
-            if ((locked >> i) & 1u) c.meta[tx.requests[i].key].fetch_and(~kLock, std::memory_order_acq_rel);
+            if ((locked >> i) & 1ull) c.meta[c.req(t, i).key].fetch_and(~kLock, std::memory_order_acq_rel);
         return false;
     }
     for (uint32_t i = 0; i < n; ++i)
-        if (!tx.requests[i].read)
-            c.write_op(tx.requests[i].key, t, i, src_image(tx, i, imgs, c.words, zero));
+        if (!c.is_read(t, i)) dg += c.write_op(t, i, src_image(c, t, i, imgs, zero));
     for (uint32_t i = 0; i < n; ++i)
-        if (!tx.requests[i].read)
-            c.meta[tx.requests[i].key].store(TICTOC ? (cts & wmask) : cts, std::memory_order_release);
+        if (!c.is_read(t, i))
+            c.meta[c.req(t, i).key].store(TICTOC ? (cts & wmask) : cts, std::memory_order_release);
     if (c.log) c.log[t] = TICTOC ? gcc_commit_rec{cts, seqv} : gcc_commit_rec{seqv, 0};
     c.digests[t] = dg;
     return true;
 }
 
-}  // namespace
-
-extern "C" int oracle_cpu_run(const char *scheme, uint8_t *table, uint64_t rows, int32_t layout,
-                              const gcc_ycsb_tx *txs, uint64_t n_tx, int32_t write_mode,
-                              uint64_t write_seed, int32_t threads, uint64_t *digests,
-                              gcc_commit_rec *commit_log, double *seconds, uint64_t *aborts) {
-    std::string s = scheme ? scheme : "";
-    int kind = s == "tpl_nw" ? 0 : s == "silo" ? 1 : s == "tictoc" ? 2 : -1;
-    if (kind < 0 || !table || !digests) return GCC_EINVAL;
-    for (uint64_t t = 0; t < n_tx; ++t) {
-        if (txs[t].request_cnt > 16) return GCC_EFORMAT;
-        for (uint32_t i = 0; i < txs[t].request_cnt; ++i)
-            if (txs[t].requests[i].key >= rows) return GCC_EKEY;
-    }
-    std::vector<std::atomic<uint64_t>> meta(rows);
+// The executor loop shared by both record formats.
+int cpu_execute(Cpu &c, int kind, int32_t threads, double *seconds, uint64_t *aborts) {
+    std::vector<std::atomic<uint64_t>> meta(c.rows);
     for (auto &m : meta) m.store(0, std::memory_order_relaxed);
-    Cpu c;
-    c.table = table;
-    c.rows = rows;
-    c.rb = rbytes(layout);
-    c.words = c.rb / 8;
-    c.write_mode = write_mode;
-    c.wseed = write_seed;
     c.meta = meta.data();
-    c.txs = txs;
-    c.n_tx = n_tx;
-    c.digests = digests;
-    c.log = commit_log;
+    const uint64_t n_tx = c.n_tx;
     unsigned nt = threads > 0 ? (unsigned)threads : std::max(1u, std::thread::hardware_concurrency());
     std::atomic<uint64_t> next{0}, ab{0};
     auto t0 = std::chrono::steady_clock::now();
     auto worker = [&]() {
-        std::vector<uint64_t> imgs(16 * c.words), zero(c.words, 0);
+        std::vector<uint64_t> imgs((size_t)kCpuMaxReq * c.words), zero(c.words, 0);
         uint64_t my_ab = 0;
         while (true) {
             uint64_t t = next.fetch_add(1);
@@ -524,6 +545,75 @@ extern "C" int oracle_cpu_run(const char *scheme, uint8_t *table, uint64_t rows,
     if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
     if (aborts) *aborts = ab.load();
     return GCC_OK;
+}
+
+int scheme_kind(const char *scheme) {
+    std::string s = scheme ? scheme : "";
+    return s == "tpl_nw" ? 0 : s == "silo" ? 1 : s == "tictoc" ? 2 : -1;
+}
+
+}  // namespace
+
+extern "C" int oracle_cpu_run(const char *scheme, uint8_t *table, uint64_t rows, int32_t layout,
+                              const gcc_ycsb_tx *txs, uint64_t n_tx, int32_t write_mode,
+                              uint64_t write_seed, int32_t threads, uint64_t *digests,
+                              gcc_commit_rec *commit_log, double *seconds, uint64_t *aborts) {
+    const int kind = scheme_kind(scheme);
+    if (kind < 0 || !table || !digests) return GCC_EINVAL;
+    for (uint64_t t = 0; t < n_tx; ++t) {
+        if (txs[t].request_cnt > 16) return GCC_EFORMAT;
+        for (uint32_t i = 0; i < txs[t].request_cnt; ++i)
+            if (txs[t].requests[i].key >= rows) return GCC_EKEY;
+    }
+    Cpu c;
+    c.table = table;
+    c.rows = rows;
+    c.rb = rbytes(layout);
+    c.words = c.rb / 8;
+    c.write_mode = write_mode;
+    c.wseed = write_seed;
+    c.txs = txs;
+    c.n_tx = n_tx;
+    c.digests = digests;
+    c.log = commit_log;
+    return cpu_execute(c, kind, threads, seconds, aborts);
+}
+
+extern "C" int oracle_cpu_run_var(const char *scheme, uint8_t *table, uint64_t rows,
+                                  int32_t layout, const uint32_t *tx_off,
+                                  const gcc_ycsb_req *reqs, uint64_t n_tx, int32_t write_mode,
+                                  uint64_t write_seed, int32_t ext_ops, int32_t threads,
+                                  uint64_t *digests, gcc_commit_rec *commit_log, double *seconds,
+                                  uint64_t *aborts) {
+    const int kind = scheme_kind(scheme);
+    if (kind < 0 || !table || !digests || !tx_off || (!reqs && n_tx)) return GCC_EINVAL;
+    const uint32_t words = rbytes(layout) / 8;
+    for (uint64_t t = 0; t < n_tx; ++t) {
+        if (tx_off[t + 1] < tx_off[t] || tx_off[t + 1] - tx_off[t] > kCpuMaxReq) return GCC_EFORMAT;
+        for (uint32_t i = tx_off[t]; i < tx_off[t + 1]; ++i) {
+            if (reqs[i].key >= rows) return GCC_EKEY;
+            if (ext_ops && reqs[i].read < 0) {
+                const uint32_t w = (uint32_t)reqs[i].read, op = (w >> 28) & 7u, f = (w >> 24) & 15u;
+                const uint32_t fmax = op == GCC_OP_STOCK ? 6u : (op == GCC_OP_PAY ? 7u : 9u);
+                if (op < GCC_OP_ADD || op > GCC_OP_INSERT || f > fmax || words != 11u)
+                    return GCC_EFORMAT;
+            }
+        }
+    }
+    Cpu c;
+    c.table = table;
+    c.rows = rows;
+    c.rb = rbytes(layout);
+    c.words = words;
+    c.write_mode = write_mode;
+    c.wseed = write_seed;
+    c.ext = ext_ops != 0;
+    c.tx_off = tx_off;
+    c.reqs = reqs;
+    c.n_tx = n_tx;
+    c.digests = digests;
+    c.log = commit_log;
+    return cpu_execute(c, kind, threads, seconds, aborts);
 }
 
 // Generator restated from generation/gen_ycsb.cu:76-152 (see oracle.h); the

@@ -87,6 +87,15 @@ int oracle_cpu_run(const char *scheme, uint8_t *table, uint64_t rows, int32_t la
                    uint64_t write_seed, int32_t threads, uint64_t *digests,
                    gcc_commit_rec *commit_log, double *seconds, uint64_t *aborts);
 
+/* The same executors over variable-length transactions (CSR, at most 64
+ * requests), with extended ops (ext_ops != 0) applied under the
+ * transaction's exclusive access like the engine does. */
+int oracle_cpu_run_var(const char *scheme, uint8_t *table, uint64_t rows, int32_t layout,
+                       const uint32_t *tx_off, const gcc_ycsb_req *reqs, uint64_t n_tx,
+                       int32_t write_mode, uint64_t write_seed, int32_t ext_ops, int32_t threads,
+                       uint64_t *digests, gcc_commit_rec *commit_log, double *seconds,
+                       uint64_t *aborts);
+
 /* Independent restatement of the dataset generator (gen_ycsb semantics). */
 int oracle_gen_ycsb(uint64_t rows, uint64_t n_tx, double theta, double read_ratio,
                     uint64_t seed, int32_t dedup, int32_t key_base, gcc_ycsb_tx *out);

@@ -41,6 +41,8 @@ def lib():
             "oracle_cpu_run": [C.c_char_p, P, U64, I32, P, U64, I32, U64, I32, P, P,
                                C.POINTER(C.c_double), C.POINTER(U64)],
             "oracle_gen_ycsb": [U64, U64, C.c_double, C.c_double, U64, I32, I32, P],
+            "oracle_cpu_run_var": [C.c_char_p, P, U64, I32, P, P, U64, I32, U64, I32, I32, P, P,
+                                   C.POINTER(C.c_double), C.POINTER(U64)],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -139,6 +141,24 @@ def cpu_run(scheme, table, layout, txs, write_mode, write_seed, threads=0, commi
                               C.byref(aborts))
     if rc != 0:
         raise RuntimeError(f"oracle_cpu_run failed: {rc}")
+    return t, dg, log, secs.value, aborts.value
+
+
+def cpu_run_var(scheme, table, layout, tx_off, reqs, write_mode, write_seed, ext_ops=False,
+                threads=0, commit_log=True):
+    """Multi-threaded CPU execution of variable-length transactions."""
+    t = np.array(table, dtype=np.uint8, copy=True)
+    tx_off = np.ascontiguousarray(tx_off, dtype=np.uint32)
+    reqs = np.ascontiguousarray(reqs)
+    n = len(tx_off) - 1
+    dg = np.zeros(n, dtype=np.uint64)
+    log = np.zeros((n, 2), dtype=np.uint64) if commit_log else None
+    secs, aborts = C.c_double(), C.c_uint64()
+    rc = lib().oracle_cpu_run_var(scheme.encode(), _p(t), t.shape[0], layout, _p(tx_off), _p(reqs),
+                                  n, write_mode, write_seed, 1 if ext_ops else 0, threads, _p(dg),
+                                  _p(log), C.byref(secs), C.byref(aborts))
+    if rc != 0:
+        raise RuntimeError(f"oracle_cpu_run_var failed: {rc}")
     return t, dg, log, secs.value, aborts.value
 
 

@@ -61,3 +61,23 @@ def test_generator_prefix_property():
     assert np.array_equal(reqs_a, reqs_b[:int(off_a[-1])])
     assert np.array_equal(kind_a, kind_b[:3000])
     assert lay_a["inserts"] == lay_b["inserts"] and lay_a["rows"] < lay_b["rows"]
+
+
+import pytest
+
+
+@pytest.mark.parametrize("scheme", ["tpl_nw", "silo", "tictoc"])
+def test_cpu_executors_on_order_entry(oracle, scheme):
+    # the multi-threaded CPU executors (the timed CPU baseline of the
+    # order-entry workload) are serializable: their commit order replays to
+    # the same table and digests
+    d = g.order_entry_desc(warehouses=2, districts=4, customers=50, items=500)
+    off, reqs, kind, lay = g.gen_order_entry(d, 3000, seed=8)
+    init = oracle.fill_table(lay["rows"], g.LAYOUT_U64X11, 5)
+    t, dg, log, secs, aborts = oracle.cpu_run_var(scheme, init, g.LAYOUT_U64X11, off, reqs,
+                                                  g.WRITE_FIELD, 3, ext_ops=True, threads=4)
+    order = oracle.commit_order(log)
+    ref_t, ref_dg = oracle.replay_var(init, g.LAYOUT_U64X11, off, reqs, order, g.WRITE_FIELD, 3,
+                                      ext_ops=True)
+    assert np.array_equal(t, ref_t) and np.array_equal(dg, ref_dg)
+    assert secs > 0
