@@ -75,6 +75,9 @@ def parse():
     ap.add_argument("--bs", type=int, default=32)
     ap.add_argument("--index", default="hash", choices=["hash", "sorted", "direct"])
     ap.add_argument("--no-reset", action="store_true")
+    ap.add_argument("--no-queue", action="store_true",
+                    help="plain workload: one launch per batch (the reference's loop) "
+                         "instead of the device queue")
     ap.add_argument("--cpu-threads", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweep", default="tpl_wd,to,mvcc,silo,tictoc,gacco,gputx",
@@ -134,7 +137,7 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "50"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (FileNotFoundError, OSError):
             self.proc = None
 
@@ -188,13 +191,29 @@ def config_of(a):
         "write": "fresh uint64 into one uniform field", "index": a.index,
         "l2": "inputs larger than L2 (1.0 GB table + 143 MB transactions > 126 MB L2)",
         "parallelism": f"replicas x{a.gpus}",
+        "execution": ("one launch per batch (the reference's batch loop)" if not use_queue(a)
+                      else "device queue: one persistent launch drains the batches of "
+                           f"{a.batch} in order (GCC_F_QUEUE)"),
     }
 
 
+# Schemes whose plain runs go through the device queue by default: measured
+# on B200 at theta 0.6 (10,485,760 rows, 1,048,576 transactions) the queue
+# gives silo 205 -> 237 M and tictoc 206 -> 255 M tx/s; 2PL loses with it
+# (tpl_nw 67 -> 46 M: without the batch barrier the hot rows' writers find
+# readers in flight at every moment and starve longer) and TO is even.
+QUEUE_DEFAULT = ("silo", "tictoc")
+
+
+def use_queue(a, scheme=None):
+    return not a.no_queue and (scheme or a.scheme) in QUEUE_DEFAULT
+
+
 def cpu_baseline(g, o, txs, a, threads):
-    """The CPU executor (oracle port of the CC rules) on the host cores, on a
-    bounded sample of the same workload."""
-    n = len(txs)  # the whole workload, one pass (well under a second per step)
+    """The CPU executor (oracle port of the CC rules) on the host cores: one
+    pass over the whole workload (a fraction of a second to a few seconds on
+    16 threads)."""
+    n = len(txs)
     sample = txs[:n]
     init = o.fill_table(a.rows, 0, 141919810)
     sch = a.scheme if a.scheme in ("tpl_nw", "silo", "tictoc") else "tpl_nw"
@@ -208,14 +227,14 @@ def cpu_baseline(g, o, txs, a, threads):
 
 
 def run_reference(a):
-    """--impl reference: the CPU port of the path on the host cores."""
+    """--impl reference: the CPU port of the path on the host cores. It uses
+    nothing of the engine: inputs come from the oracle's own generator (the
+    same records as the engine's for the same seed)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import gpu_cc_tb_b200 as g
     from oracle import oracle_py as o
-    txs = g.gen_ycsb(a.rows, a.txs, a.theta, a.read_ratio, seed=141919810,
-                     dedup=g.DEDUP_RESAMPLE, key_base=0)
+    txs = o.gen_ycsb(a.rows, a.txs, a.theta, a.read_ratio, 141919810, 1, 0)  # dedup resample
     threads = a.cpu_threads or os.cpu_count()
     sch = a.scheme if a.scheme in ("tpl_nw", "silo", "tictoc") else "tpl_nw"
     n = len(txs)
@@ -223,7 +242,7 @@ def run_reference(a):
     times = []
     for step in range(a.warmup + a.steps):
         sample = txs[(step * n) % len(txs):][:n]
-        _, _, _, secs, _ = o.cpu_run(sch, init, 0, sample, g.WRITE_FIELD, 1, threads=threads,
+        _, _, _, secs, _ = o.cpu_run(sch, init, 0, sample, 0, 1, threads=threads,  # field writes
                                      commit_log=False)
         if step >= a.warmup:
             times.append(secs)
@@ -643,7 +662,7 @@ def main():
     eng = g.Engine(a.rows, layout=g.LAYOUT_U64X11, index=index, fill_seed=141919810,
                    device=local, max_batch=a.batch)
     eng.load_txs(host_txs)
-    flags = g.F_NO_RESET if a.no_reset else 0
+    flags = (g.F_NO_RESET if a.no_reset else 0) | (g.F_QUEUE if use_queue(a) else 0)
     kw = dict(warp_density=a.wd, block_size=a.bs, batch_size=a.batch, flags=flags, write_seed=1)
     for _ in range(a.warmup):
         eng.run(a.scheme, **kw)
@@ -667,12 +686,11 @@ def main():
         n_tx_launches = r["batches"]
     wall = time.perf_counter() - t0
     replicas.barrier(dist)
-    clk = clocks.stop()
 
     # end to end through the public API: H2D of the step's transactions from
     # pinned memory, the run, D2H of every transaction's read digest; the
     # engine overlaps each batch's copies with the other batches' execution
-    # (gcc_run_host)
+    # (gcc_run_host). The clock record covers both timed regions.
     for _ in range(a.warmup):
         eng.run_host(a.scheme, host_txs, digests_host, **kw)
     e2e_s = 0.0
@@ -681,6 +699,7 @@ def main():
         s0 = time.perf_counter()
         eng.run_host(a.scheme, host_txs, digests_host, **kw)
         e2e_s += time.perf_counter() - s0
+    clk = clocks.stop()
 
     job = replicas.combine(dist, dev_s, committed, e2e_s, a.steps * a.txs)
     dev_s_max, value, e2e_val = job["device_s_max"], job["value"], job["e2e_value"]
@@ -734,13 +753,26 @@ def main():
                                "tx_per_s": statistics.median(r["tx_per_s"] for r in rs),
                                "kernel_ms": kms, "achieved_gbs": ach, "frac_of_hbm": ach / hbm,
                                "note": "one launch of 65,536 transactions at low contention"}
+        if use_queue(a):
+            # the same workload with one launch per batch, for comparison
+            ks = dict(kw, flags=kw["flags"] & ~g.F_QUEUE)
+            eng.run(a.scheme, **ks)
+            rs = [eng.run(a.scheme, **ks) for _ in range(3)]
+            line["per_batch_launches"] = {
+                "tx_per_s": statistics.median(r["tx_per_s"] for r in rs),
+                "launches": rs[0]["batches"],
+                "note": "same workload, one kernel launch per 65,536-transaction batch"}
         if a.sweep:
             sw = {}
             for s in a.sweep.split(","):
-                eng.run(s, **kw)          # first run sizes the scheme's buffers
-                r = eng.run(s, **kw)
+                fl = kw["flags"] & ~g.F_QUEUE
+                if use_queue(a, s):
+                    fl |= g.F_QUEUE
+                ks = dict(kw, flags=fl)
+                eng.run(s, **ks)          # first run sizes the scheme's buffers
+                r = eng.run(s, **ks)
                 sw[s] = {"tx_per_s": r["tx_per_s"], "aborts": r["aborts"],
-                         "p99_us": r["lat_p99_us"]}
+                         "p99_us": r["lat_p99_us"], "queue": bool(fl & g.F_QUEUE)}
             line["sweep"] = sw
         print(json.dumps(line), flush=True)
     eng.close()

@@ -39,6 +39,9 @@ INDEX_HASH, INDEX_SORTED, INDEX_DIRECT = 0, 1, 2
 WRITE_FIELD, WRITE_ROWCOPY = 0, 1
 F_COMMIT_LOG, F_READ_LOG, F_NO_RESET, F_RETRY_IMMEDIATE = 1, 2, 4, 8
 F_AUTOTUNE, F_GRAPH = 16, 32
+F_QUEUE = 128  # gcc_run / gcc_run_host: all batches through one device-queue launch
+QUEUE_SCHEMES = ("tpl_nw", "tpl_wd", "to", "silo", "tictoc", "slow_tpl_nw", "slow_tpl_wd",
+                 "slow_to", "slow_silo", "slow_tictoc")
 BATCHES_SEQUENTIAL, BATCHES_QUEUE = 0, 1
 DEDUP_DROP, DEDUP_RESAMPLE = 0, 1
 
@@ -160,6 +163,17 @@ SCHED_FEAT_STRIDE = 72
 SCHED_SCHEMES = ["tpl_nw", "tpl_wd", "silo", "tictoc"]
 
 
+CALIB_ADD, CALIB_CAS = 0, 1
+
+
+def l2_atomic_rate(device: int = 0, words: int = 1 << 23, mode: int = CALIB_ADD) -> float:
+    """64-bit L2 atomics per second the device sustains on pseudo-random words
+    of a `words`-word array (gcc_l2_atomic_rate)."""
+    r = C.c_double()
+    _check(library().gcc_l2_atomic_rate(device, words, mode, C.byref(r)), "gcc_l2_atomic_rate")
+    return r.value
+
+
 def library_path() -> Path:
     return Path(os.environ.get("GCC_LIB", LIB_PATH))
 
@@ -199,6 +213,8 @@ def library() -> C.CDLL:
         "gcc_get_read_log": (C.c_int, [P, P, C.c_uint64]),
         "gcc_index_lookup": (C.c_int, [P, P, P, C.c_uint64]),
         "gcc_last_kernel_ms": (C.c_int, [P, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
+        "gcc_l2_atomic_rate": (C.c_int, [C.c_int32, C.c_uint64, C.c_int32,
+                                         C.POINTER(C.c_double)]),
         "gcc_gen_ycsb_var_offsets": (C.c_int, [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, P]),
         "gcc_gen_ycsb_var": (C.c_int, [C.c_uint64, C.c_uint64, C.c_double, C.c_double,
                                        C.c_uint64, C.c_int32, C.c_int32, P, P]),

@@ -1255,7 +1255,12 @@ __global__ void __launch_bounds__(1024, 1) ycsb_kernel(const __grid_constant__ K
         uint32_t beg = 0;
         if constexpr (MO == kMaxOps) {
             T = p.txs + tx;
-            n64 = __ldg(&T->request_cnt);
+            // With a device queue the records of later batches are still
+            // being copied in while earlier ones run: read them through L2
+            // (a line cached in L1 next to an earlier record could predate
+            // the copy).
+            n64 = p.queue_tail ? __ldcg((const unsigned long long *)&T->request_cnt)
+                               : __ldg(&T->request_cnt);
         } else {
             beg = __ldg(p.tx_off + tx);
             n64 = (unsigned long long)(__ldg(p.tx_off + tx + 1) - beg);
@@ -1274,7 +1279,9 @@ __global__ void __launch_bounds__(1024, 1) ycsb_kernel(const __grid_constant__ K
             s.row[k] = kNoRow;
             if (i < s.n) {
                 int2 rq;
-                if constexpr (MO == kMaxOps) rq = __ldg((const int2 *)&T->requests[i]);
+                if constexpr (MO == kMaxOps)
+                    rq = p.queue_tail ? __ldcg((const int2 *)&T->requests[i])
+                                      : __ldg((const int2 *)&T->requests[i]);
                 else rq = __ldg((const int2 *)(p.reqs + beg + i));
                 s.valid |= 1u << k;
                 if (rq.x > 0) { s.isread |= 1u << k; myreads |= 1ull << i; }

@@ -76,6 +76,16 @@ double hist_percentile_us(const Counters &hc, double q) {
 uint32_t starve_param(int32_t v) { return v < 0 ? 0u : (v == 0 ? 32u : (uint32_t)v); }
 
 bool is_slow(int s) { return s >= S_SLOW_TPL_NW; }
+// Schemes whose CC metadata stays valid from one batch to the next, so that
+// batches can share one launch (GCC_F_QUEUE): 2PL releases every lock,
+// Silo / TicToc words only grow, TO timestamps keep growing when the
+// counter is not reset. Not MVCC (its version store is indexed by batch
+// position) nor the ordered schemes (per-batch ordering passes).
+bool queue_scheme(int s) {
+    return s == S_TPL_NW || s == S_TPL_WD || s == S_TO || s == S_SILO || s == S_TICTOC ||
+           s == S_SLOW_TPL_NW || s == S_SLOW_TPL_WD || s == S_SLOW_TO || s == S_SLOW_SILO ||
+           s == S_SLOW_TICTOC;
+}
 bool uses_ts(int s) { return s == S_TO || s == S_SLOW_TO || s == S_MVCC || s == S_SLOW_MVCC; }
 bool is_mvcc(int s) { return s == S_MVCC || s == S_SLOW_MVCC; }
 
@@ -174,6 +184,8 @@ struct gcc_engine {
     uint64_t n_var = 0, var_ops = 0, cap_var = 0, cap_var_ops = 0;
     std::vector<uint32_t> tx_off_h;  // host copy of the offsets (batch classes)
     unsigned long long *queue_tail = nullptr;
+    uint64_t *tail_h = nullptr;  // pinned: queue tail after each batch (GCC_F_QUEUE)
+    uint64_t tail_cap = 0;
     unsigned long long *stamps = nullptr;  // device time stamps of batched runs
     uint64_t stamps_cap = 0;
     struct Arm {
@@ -243,6 +255,7 @@ gcc_engine::~gcc_engine() {
     for (uint32_t *t : scan_tmp)
         if (t) cudaFree(t);
     for (cudaEvent_t ev : events) cudaEventDestroy(ev);
+    if (tail_h) cudaFreeHost(tail_h);
     if (graph) cudaGraphExecDestroy(graph);
     if (copy_in) cudaStreamDestroy(copy_in);
     if (copy_out) cudaStreamDestroy(copy_out);
@@ -611,6 +624,10 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
     const uint64_t nbatches = (e->n_tx + batch - 1) / batch;
     const bool rowcopy = rp->write_mode == GCC_WRITE_ROWCOPY;
     const bool want_log = (rp->flags & GCC_F_READ_LOG) != 0;
+    // GCC_F_QUEUE: one persistent launch drains every batch in order
+    const bool queue = (rp->flags & GCC_F_QUEUE) != 0;
+    if (queue && (!queue_scheme(s) || rowcopy)) return GCC_EINVAL;
+    const uint64_t nlaunch = queue ? 1 : nbatches;
     int rc;
 
     // lazily sized per-run buffers
@@ -664,6 +681,25 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
     if ((rc = e->ensure_events(3 * nbatches + 4 + (streamed ? 2 * nbatches : 0)))) return rc;
     cudaEvent_t ev_start = e->events[0], ev_pre0 = e->events[1], ev_stop = e->events[2];
     const uint64_t launches0 = e->kernel_launches;
+    if (queue && streamed) {
+        // the device queue's tail, and the pinned host values the copy
+        // stream writes into it after each batch's records
+        if (!e->queue_tail && (rc = e->alloc(&e->queue_tail, 8))) return rc;
+        if (e->tail_cap < nbatches) {
+            if (e->tail_h) cudaFreeHost(e->tail_h);
+            e->tail_h = nullptr;
+            e->tail_cap = 0;
+            cudaError_t he = cudaHostAlloc((void **)&e->tail_h, nbatches * 8, cudaHostAllocDefault);
+            if (he != cudaSuccess) {
+                e->tail_h = nullptr;
+                cudaGetLastError();
+                return GCC_ENOMEM;
+            }
+            e->tail_cap = nbatches;
+        }
+        for (uint64_t b = 0; b < nbatches; ++b)
+            e->tail_h[b] = std::min<uint64_t>((b + 1) * batch, e->n_tx);
+    }
 
     cudaStream_t st = e->stream;
     cudaError_t ce;
@@ -673,10 +709,14 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
         if (ce != cudaSuccess) return e->fail_cuda(ce); \
     } while (0)
     CKR(cudaMemsetAsync(e->ctr, 0, sizeof(Counters), st));
+    // (before ev_start: the copy stream's tail updates come after this)
+    if (queue && streamed) CKR(cudaMemsetAsync(e->queue_tail, 0, 8, st));
     CKR(cudaEventRecord(ev_start, st));
     if (streamed) {
         // host records stream in batch by batch on their own stream; each
-        // batch waits only for its own records (gcc_run_host)
+        // batch waits only for its own records (gcc_run_host); with the
+        // device queue, each copy is followed by the queue tail's advance
+        // past that batch
         if (!e->copy_in) CKR(cudaStreamCreateWithFlags(&e->copy_in, cudaStreamNonBlocking));
         if (!e->copy_out) CKR(cudaStreamCreateWithFlags(&e->copy_out, cudaStreamNonBlocking));
         CKR(cudaStreamWaitEvent(e->copy_in, ev_start, 0));
@@ -684,6 +724,9 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
             const uint64_t bst = b * batch, bn = std::min<uint64_t>(batch, e->n_tx - bst);
             CKR(cudaMemcpyAsync(e->txs + bst, e->host_src + bst, bn * sizeof(gcc_ycsb_tx),
                                 cudaMemcpyHostToDevice, e->copy_in));
+            if (queue)
+                CKR(cudaMemcpyAsync(e->queue_tail, e->tail_h + b, 8, cudaMemcpyHostToDevice,
+                                    e->copy_in));
             CKR(cudaEventRecord(e->events[ev_copy + b], e->copy_in));
         }
     }
@@ -694,14 +737,17 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
         p.order = e->order;
     }
     CKR(cudaEventRecord(ev_pre0, st));
-    for (uint64_t b = 0; b < nbatches; ++b) {
+    for (uint64_t b = 0; b < nlaunch; ++b) {
         cudaEvent_t e0 = e->events[3 + 3 * b], e1 = e->events[4 + 3 * b], e2 = e->events[5 + 3 * b];
         const uint64_t bst = b * batch;
-        const uint64_t bn = std::min<uint64_t>(batch, e->n_tx - bst);
+        // queue: the launch covers every position; batches are admitted
+        // through the queue tail (streamed) or all at once
+        const uint64_t bn = queue ? e->n_tx : std::min<uint64_t>(batch, e->n_tx - bst);
         p.batch_st = (uint32_t)bst;
         p.batch_n = (uint32_t)bn;
+        p.queue_tail = (queue && streamed) ? e->queue_tail : nullptr;
         CKR(cudaEventRecord(e0, st));
-        if (streamed) CKR(cudaStreamWaitEvent(st, e->events[ev_copy + b], 0));
+        if (streamed && !queue) CKR(cudaStreamWaitEvent(st, e->events[ev_copy + b], 0));
         // per-batch metadata reset (the reference memsets the whole table).
         // 2PL lock words are all zero again once a batch has committed every
         // transaction (each lock taken is released), so for 2PL the memset
@@ -734,6 +780,7 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
         CKR(cudaEventRecord(e2, st));
         if (streamed && e->host_dg) {
             // the batch's read digests go back while later batches run
+            // (queue: all of them after the one launch)
             CKR(cudaStreamWaitEvent(e->copy_out, e2, 0));
             CKR(cudaMemcpyAsync(e->host_dg + bst, e->digest + bst, bn * 8, cudaMemcpyDeviceToHost,
                                 e->copy_out));
@@ -755,7 +802,7 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
     double pre_ms = 0, proc_ms = 0;
     cudaEventElapsedTime(&ms, ev_start, ev_pre0);
     pre_ms += ms;
-    for (uint64_t b = 0; b < nbatches; ++b) {
+    for (uint64_t b = 0; b < nlaunch; ++b) {
         cudaEventElapsedTime(&ms, e->events[3 + 3 * b], e->events[4 + 3 * b]);
         pre_ms += ms;
         cudaEventElapsedTime(&ms, e->events[4 + 3 * b], e->events[5 + 3 * b]);
@@ -764,7 +811,7 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
     cudaEventElapsedTime(&ms, ev_start, ev_stop);
     double tot_ms = ms;
     e->last_kernel_ms = proc_ms;
-    e->last_launches = nbatches;
+    e->last_launches = nlaunch;
 
     out->committed = hc.committed;
     out->aborts = hc.aborts;
@@ -780,7 +827,7 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
     out->tot_d = hc.tot_cycles * inv;
     out->idx_d = hc.idx_cycles * inv;
     out->rank_count = gputx ? hc.max_rank + 1 : 0;
-    out->batches = nbatches;
+    out->batches = nlaunch;
     out->kernel_launches = e->kernel_launches - launches0;
     out->max_attempts = hc.max_attempts;
     out->err_site = hc.err_where;

@@ -78,6 +78,21 @@ extern "C" {
 #define GCC_F_EXT_OPS 64u   /* requests with a negative `read` word are
                                extended ops (GCC_OP_*); without this flag
                                every request with read <= 0 is a YCSB write */
+#define GCC_F_QUEUE 128u    /* gcc_run / gcc_run_host: the batches go through
+                               ONE persistent launch that takes positions in
+                               batch order from a device queue, instead of one
+                               launch per batch with a barrier between
+                               batches (the reference's loop, benchmark_cpu/
+                               ycsb.cu:262-285), so batch b+1's first
+                               transactions fill the SMs that batch b's retry
+                               tail leaves idle. gcc_run admits every batch at
+                               once; gcc_run_host admits batch b when its
+                               records have reached the device. The CC
+                               metadata and the timestamp counter are reset
+                               once per run, not per batch. Schemes whose
+                               metadata stays valid across batches: tpl_nw,
+                               tpl_wd, to, silo, tictoc and their slow_
+                               variants; GCC_WRITE_FIELD only. */
 
 /* ---- extended request ops ------------------------------------------------
  * A request whose `read` word is negative is an integer write op on the u64
@@ -355,9 +370,12 @@ int gcc_index_lookup(gcc_engine *e, const uint32_t *keys, uint32_t *rows,
  * library until exit; larger tables are rejected with GCC_EINVAL. Calls on a
  * device share that array and clear it before use, so calls that overlap on
  * the GPU race. The first call on a device looks up the array's address with
- * the device current; make it before any stream capture. Runs on `stream`
- * (a cudaStream_t, may be null) and waits for it; committed / aborts may be
- * null. */
+ * the device current; make it before any stream capture. The address belongs
+ * to the device's primary context: after cudaDeviceReset the entry point
+ * must not be called on that device again in the process. Runs on `stream`
+ * (a cudaStream_t, may be null) and returns only after its kernel has
+ * finished, on errors too; committed / aborts may be null. Retries follow
+ * gcc_run's defaults (starvation control at 32 attempts). */
 int gcc_run_tpl_nw_noalloc(const gcc_ycsb_tx *txs, uint64_t n_tx, void *table,
                            uint64_t rows, uint64_t *digests, uint32_t *tx_aborts,
                            uint64_t write_seed, void *stream, uint64_t *committed,
@@ -376,6 +394,17 @@ int gcc_run_host(gcc_engine *e, const gcc_run_params *p, const gcc_ycsb_tx *host
 /* Device-side timing of the last run's main kernels: total ms and number of
  * launches of the transaction kernel (for roofline accounting). */
 int gcc_last_kernel_ms(gcc_engine *e, double *kernel_ms, uint64_t *launches);
+
+/* L2 atomic throughput of `device` on the CC metadata's access pattern (no
+ * counterpart in the reference): every SM issues 64-bit atomics to
+ * pseudo-random words of a `words`-word array (a power of two, 1,024 ..
+ * 16,777,216 words, i.e. at most 128 MiB, about the L2), 8 in flight per
+ * thread; *atomics_per_s = atomics completed per second of the timed pass.
+ * The denominator of the transaction kernel's L2 atomic rate (ncu
+ * lts__t_requests_op_atom + _op_red). Allocates and frees its array. */
+#define GCC_CALIB_ADD 0
+#define GCC_CALIB_CAS 1
+int gcc_l2_atomic_rate(int32_t device, uint64_t words, int32_t mode, double *atomics_per_s);
 
 /* ---- Learned contention scheduling (no counterpart in the reference,
  * which runs every batch in transaction-index order with one launch,

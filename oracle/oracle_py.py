@@ -162,9 +162,41 @@ def cpu_run_var(scheme, table, layout, tx_off, reqs, write_mode, write_seed, ext
     return t, dg, log, secs.value, aborts.value
 
 
+# gen_ycsb record: {uint64 request_cnt; {int32 read; uint32 key}[16]} = 136 B
+# (include/ycsb.cuh:21-33 of the reference)
+TX_DTYPE = np.dtype([("request_cnt", "<u8"),
+                     ("requests", np.dtype([("read", "<i4"), ("key", "<u4")]), (16,))])
+
+
 def gen_ycsb(rows, n_tx, theta, read_ratio, seed, dedup, key_base):
-    from gpu_cc_tb_b200 import TX_DTYPE
+    """The oracle's restatement of the dataset generator (same records as
+    the engine's gcc_gen_ycsb for the same arguments)."""
     out = np.zeros(n_tx, dtype=TX_DTYPE)
     rc = lib().oracle_gen_ycsb(rows, n_tx, theta, read_ratio, seed, dedup, key_base, _p(out))
     assert rc == 0, rc
     return out
+
+
+_M64 = (1 << 64) - 1
+
+
+def _sm64(x):
+    z = (x + 0x9E3779B97F4A7C15) & _M64
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & _M64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & _M64
+    return z ^ (z >> 31)
+
+
+def _h3(s, a, b):
+    return _sm64(_sm64(s ^ ((a * 0x9E3779B97F4A7C15) & _M64)) ^ ((b * 0xC2B2AE3D27D4EB4F) & _M64))
+
+
+def write_field(write_seed, tx, op):
+    """Field (0..9) a GCC_WRITE_FIELD write request `op` of transaction `tx`
+    stores into (the formula oracle.cpp's replay applies)."""
+    return _h3(write_seed, tx, 2 * op) % 10
+
+
+def write_value(write_seed, tx, op):
+    """Value that write request `op` of transaction `tx` stores."""
+    return _h3(write_seed, tx, 2 * op + 1)
