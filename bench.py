@@ -80,6 +80,10 @@ def parse():
                          "instead of the device queue")
     ap.add_argument("--cpu-threads", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the learned-vs-plain comparison at theta 0.99")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own GPU build (oracle/_ref)")
     ap.add_argument("--sweep", default="tpl_wd,to,mvcc,silo,tictoc,gacco,gputx",
                     help="comma list of extra schemes timed once on the same workload "
                          "('' for none)")
@@ -224,6 +228,113 @@ def cpu_baseline(g, o, txs, a, threads):
             "kind": "port", "scheme": sch,
             "sample": f"first {n} of the {len(txs)} transactions, one pass, {nthreads} threads, "
                       f"{a.rows} rows"}, secs
+
+
+# Schemes timed against the reference's own GPU build in its own format;
+# gacco and mvcc are left out at this shape because the reference's own code
+# cannot run them there (oracle/ref_gpu.py: gacco's unbounded hand-off needs
+# every transaction of a 65,536-transaction batch resident, MVCC_CPU::Init
+# writes past its version array from the second batch on).
+REF_GPU_SCHEMES = ("tpl_nw", "tpl_wd", "to", "silo", "tictoc", "gputx", "slow_tpl_nw",
+                   "slow_tpl_wd", "slow_to", "slow_silo", "slow_tictoc")
+
+
+def reference_format_txs(a):
+    """The workload's records in the reference's own dataset semantics:
+    repeated keys dropped, keys in [1, rows-1] (generation/gen_ycsb.cu)."""
+    from oracle import oracle_py as o
+    return o.gen_ycsb(a.rows, a.txs, a.theta, a.read_ratio, 141919810, 0, 1)
+
+
+def reference_gpu_baseline(a, txs):
+    """The reference's own test_ycsb (built from its sources into
+    oracle/_ref/) on this GPU, per scheme, on `txs` in its own format: 104 B
+    rows, sorted-array index, whole-row copies, the same batch size, warp
+    density and block size. Its `through` is committed tx over its tot_time
+    (metadata resets + precompute + kernels, benchmark_cpu/ycsb.cu:249-291)."""
+    from oracle import ref_gpu
+    if not ref_gpu.available():
+        return {"unavailable": "the reference build is missing (make -C oracle ref REF=<dir>)"}
+    out = {"workload": (f"ycsb_ref104_{a.rows}rows_{a.txs}tx_theta{a.theta}_r{a.read_ratio}"
+                        f"_batch{a.batch}_wd{a.wd}_bs{a.bs}"),
+           "program": "reference test_ycsb (unmodified), NVRTC kernel JIT-compiled for sm_100",
+           "tx_per_s": {}, "aborts": {}}
+    with tempfile.TemporaryDirectory() as td:
+        ds = Path(td) / "ycsb.txs"
+        ds.write_bytes(txs.tobytes())
+        for s in REF_GPU_SCHEMES:
+            try:
+                r = ref_gpu.run(ds, a.rows, len(txs), s, a.wd, a.bs, a.batch, timeout=600)
+                out["tx_per_s"][s] = r["through"]
+                out["aborts"][s] = r.get("abort")
+            except Exception as e:  # report, do not fail the engine's line
+                out["tx_per_s"][s] = None
+                out.setdefault("errors", {})[s] = str(e)[-300:]
+    return out
+
+
+def engine_reference_format(g, a, txs, local, index_kind):
+    """The engine on the reference's format and records (the comparison
+    side of reference_gpu_baseline): 104 B rows, sorted index, whole-row
+    copies, one launch per batch."""
+    out = {"tx_per_s": {}, "aborts": {}}
+    with g.Engine(a.rows, layout=g.LAYOUT_REF104, index=g.INDEX_SORTED, fill_seed=0,
+                  device=local, max_batch=a.batch) as e:
+        e.load_txs(txs)
+        for s in REF_GPU_SCHEMES:
+            k = dict(warp_density=a.wd, block_size=a.bs, batch_size=a.batch,
+                     write_mode=g.WRITE_ROWCOPY, write_seed=1)
+            e.run(s, **k)
+            rs = [e.run(s, **k) for _ in range(3)]
+            out["tx_per_s"][s] = statistics.median(r["tx_per_s"] for r in rs)
+            out["aborts"][s] = rs[-1]["aborts"]
+    return out
+
+
+CAPS = (256, 512, 1024, 2048)
+
+
+def learned_vs_plain(g, eng, a, sch, n_batches=16, theta=0.99):
+    """BASELINE's headline comparison on the benchmark's table: n_batches
+    batches of 65,536 transactions at Zipf theta 0.99 (read ratio 0.9),
+    committed tx/s of
+      plain        the plain kernel, one launch per batch, every transaction
+                   of the batch in flight the GPU holds;
+      plain_best   the plain kernel at its best in-flight cap (max_active
+                   swept over CAPS) -- the honest denominator;
+      learned      the learned scheduler (predictor trained online, the
+                   measured policy, deferral and caps) after two training
+                   passes;
+      untrained    the same scheduler with the network left at its initial
+                   weights (train_steps -1): the ablation of the network."""
+    txs = g.gen_ycsb(a.rows, n_batches * a.batch, theta, a.read_ratio, seed=20240521,
+                     dedup=g.DEDUP_RESAMPLE, key_base=0)
+    eng.load_txs(txs)
+    kw = dict(warp_density=a.wd, block_size=a.bs, batch_size=a.batch, write_seed=1)
+    out = {"workload": f"ycsb_{a.rows}rows_{n_batches}x{a.batch}tx_16ops_theta{theta}_r{a.read_ratio}",
+           "cc_scheme": sch}
+    r = eng.run(sch, **kw)
+    out["plain"] = {"tx_per_s": r["tx_per_s"], "abort_rate": r["aborts"] / max(1, r["aborts"] + r["committed"])}
+    caps = {}
+    for c in CAPS:
+        eng.run(sch, max_active=c, **kw)
+        r = eng.run(sch, max_active=c, **kw)
+        caps[c] = r["tx_per_s"]
+    best = max(caps, key=caps.get)
+    out["plain_caps"] = caps
+    out["plain_best"] = {"max_active": best, "tx_per_s": caps[best]}
+    for name, steps in (("learned", 0), ("untrained", -1)):
+        with g.Scheduler(eng, mode=g.SCHED_LEARNED, train_steps=steps, seed=7) as sc:
+            sc.run(sch, **kw)
+            sc.run(sch, **kw)
+            r = sc.run(sch, **kw)
+            out[name] = {"tx_per_s": r["committed"] / r["tot_s"],
+                         "abort_rate": r["aborts"] / max(1, r["aborts"] + r["committed"]),
+                         "p99_us": r["lat_p99_us"]}
+    out["learned_over_plain"] = out["learned"]["tx_per_s"] / out["plain"]["tx_per_s"]
+    out["learned_over_plain_best"] = out["learned"]["tx_per_s"] / out["plain_best"]["tx_per_s"]
+    out["learned_over_untrained"] = out["learned"]["tx_per_s"] / out["untrained"]["tx_per_s"]
+    return out
 
 
 def run_reference(a):
@@ -774,6 +885,20 @@ def main():
                 sw[s] = {"tx_per_s": r["tx_per_s"], "aborts": r["aborts"],
                          "p99_us": r["lat_p99_us"], "queue": bool(fl & g.F_QUEUE)}
             line["sweep"] = sw
+        if ws == 1 and not a.no_learned and a.scheme in g.SCHED_SCHEMES:
+            line["learned_vs_plain"] = learned_vs_plain(g, eng, a, a.scheme)
+        if ws == 1 and not a.no_reference_gpu:
+            ref = reference_gpu_baseline(a, reference_format_txs(a))
+            line["reference_gpu"] = ref
+            if "tx_per_s" in ref:
+                # the same records from the engine's own generator
+                etx = g.gen_ycsb(a.rows, a.txs, a.theta, a.read_ratio, seed=141919810,
+                                 dedup=g.DEDUP_DROP, key_base=1)
+                eng_ref = engine_reference_format(g, a, etx, local, index)
+                line["engine_reference_format"] = eng_ref
+                line["vs_reference_gpu"] = {
+                    s: (eng_ref["tx_per_s"][s] / ref["tx_per_s"][s]
+                        if ref["tx_per_s"].get(s) else None) for s in REF_GPU_SCHEMES}
         print(json.dumps(line), flush=True)
     eng.close()
     if dist is not None:

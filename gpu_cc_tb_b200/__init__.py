@@ -55,7 +55,8 @@ TX_DTYPE = np.dtype([("request_cnt", "<u8"),
 assert TX_DTYPE.itemsize == 136
 REQ_DTYPE = np.dtype([("read", "<i4"), ("key", "<u4")])
 # schemes of the batched executors (gcc_run_batches); mvcc: sequential only
-VAR_SCHEMES = ("tpl_nw", "tpl_wd", "to", "silo", "tictoc", "mvcc")
+VAR_SCHEMES = ("tpl_nw", "tpl_wd", "to", "silo", "tictoc", "mvcc", "slow_tpl_nw", "slow_tpl_wd",
+               "slow_to", "slow_silo", "slow_tictoc", "slow_mvcc")
 
 
 class GccError(RuntimeError):
@@ -223,6 +224,7 @@ def library() -> C.CDLL:
                                       C.POINTER(Result)]),
         "gcc_get_batch_stats": (C.c_int, [P, P, P, P, C.c_uint64]),
         "gcc_get_batch_active": (C.c_int, [P, P, C.c_uint64]),
+        "gcc_get_batch_split": (C.c_int, [P, P, C.c_uint64]),
         "gcc_oe_offsets": (C.c_int, [C.POINTER(OeDesc), C.c_uint64, C.c_uint64, P,
                                      C.POINTER(OeLayout)]),
         "gcc_oe_gen": (C.c_int, [C.POINTER(OeDesc), C.c_uint64, C.c_uint64, C.c_int32, P, P, P]),
@@ -430,6 +432,13 @@ class Engine:
         _check(self.lib.gcc_get_batch_stats(self._h, _ptr(wd), _ptr(bs), _ptr(ms), n),
                "gcc_get_batch_stats")
         return wd, bs, ms
+
+    def batch_split(self) -> np.ndarray:
+        """batch_size (transactions per launch inside a batch, 0 = whole
+        batch) of each entry of the last run_batches."""
+        out = np.zeros(self._last_nconf, dtype=np.uint32)
+        _check(self.lib.gcc_get_batch_split(self._h, _ptr(out), len(out)), "gcc_get_batch_split")
+        return out
 
     def batch_active(self) -> np.ndarray:
         """Transactions in flight of each entry of the last run_batches."""

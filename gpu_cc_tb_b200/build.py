@@ -29,7 +29,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", str(INCLUDE)]
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-I", str(INCLUDE)]
 
-CU_UNITS = ["engine", "cc_tpl", "cc_to", "cc_mvcc", "cc_silo", "cc_tictoc", "cc_ordered", "cc_var", "sched",
+CU_UNITS = ["engine", "cc_tpl", "cc_to", "cc_mvcc", "cc_silo", "cc_tictoc", "cc_ordered", "cc_var", "cc_var_slow", "sched",
             "noalloc", "calib"]
 CXX_UNITS = ["gen", "orderentry"]
 HEADERS = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(INCLUDE.glob("*.h"))

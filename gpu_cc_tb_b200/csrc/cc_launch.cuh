@@ -63,6 +63,8 @@ int occupancy_var_one(int G, int block) {
 }
 cudaError_t launch_var(int s, int G, int grid, int block, const KParams &p, cudaStream_t st);
 int occupancy_var(int s, int G, int block);
+cudaError_t launch_var_slow(int s, int G, int grid, int block, const KParams &p, cudaStream_t st);
+int occupancy_var_slow(int s, int G, int block);
 
 // Declared per family; defined in cc_<family>.cu.
 cudaError_t launch_family_tpl(int s, int G, int grid, int block, const KParams &p, cudaStream_t st);

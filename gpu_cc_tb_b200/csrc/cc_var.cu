@@ -1,5 +1,6 @@
 // Variable-length transactions (up to 64 requests) for the batched-queue
-// executor: tpl_nw, tpl_wd, to, silo, tictoc, mvcc at G in {4, 8, 16, 32}.
+// executor: tpl_nw, tpl_wd, to, silo, tictoc, mvcc at G in {4, 8, 16, 32};
+// the latch variants are in cc_var_slow.cu.
 #include "cc_launch.cuh"
 
 namespace gcc {
@@ -12,7 +13,7 @@ cudaError_t launch_var(int s, int G, int grid, int block, const KParams &p, cuda
         case S_SILO: return launch_var_one<S_SILO>(G, grid, block, p, st);
         case S_TICTOC: return launch_var_one<S_TICTOC>(G, grid, block, p, st);
         case S_MVCC: return launch_var_one<S_MVCC>(G, grid, block, p, st);
-        default: return cudaErrorInvalidValue;
+        default: return launch_var_slow(s, G, grid, block, p, st);
     }
 }
 
@@ -24,7 +25,7 @@ int occupancy_var(int s, int G, int block) {
         case S_SILO: return occupancy_var_one<S_SILO>(G, block);
         case S_TICTOC: return occupancy_var_one<S_TICTOC>(G, block);
         case S_MVCC: return occupancy_var_one<S_MVCC>(G, block);
-        default: return -1;
+        default: return occupancy_var_slow(s, G, block);
     }
 }
 

@@ -190,6 +190,8 @@ struct gcc_engine {
     uint64_t stamps_cap = 0;
     struct Arm {
         int wd, bs, div;     // grid = the full persistent grid / div
+        uint32_t split;      // batch_size: at most this many transactions per
+                             // launch inside a batch (0: the whole batch)
         uint64_t active;     // transactions in flight under this arm
         double ms_per_tx = 0;
         uint64_t runs = 0;
@@ -200,6 +202,7 @@ struct gcc_engine {
     std::vector<int32_t> bstat_wd, bstat_bs;
     std::vector<double> bstat_ms;
     std::vector<uint64_t> bstat_active;
+    std::vector<uint32_t> bstat_split;
     // timing
     std::vector<cudaEvent_t> events;
     double last_kernel_ms = 0;
@@ -886,15 +889,21 @@ int gcc_load_var_txs(gcc_engine *e, const uint32_t *tx_off, const gcc_ycsb_req *
 
 namespace {
 
+// Schemes with variable-length kernels: every scheme but the ordered ones
+// (GaccO / GPUTx build their per-row access orders from 16-slot records).
 bool var_scheme(int s) {
-    return s == S_TPL_NW || s == S_TPL_WD || s == S_TO || s == S_SILO || s == S_TICTOC || s == S_MVCC;
+    return s != S_GACCO && s != S_GPUTX && s >= 0 && s < S_COUNT;
 }
 
-// Autotuner candidates (warp_density, block_size, grid divisor), tried in
-// this order: the densest groups first, then fewer transactions in flight,
-// then more.
-const int kArms[][3] = {{5, 32, 1}, {5, 32, 2}, {5, 32, 4}, {4, 32, 2},
-                        {5, 16, 1}, {4, 32, 1}, {3, 32, 2}, {3, 32, 1}};
+// Autotuner candidates (warp_density, block_size, grid divisor, batch_size
+// = transactions per launch inside a batch, 0 for the whole batch), tried in
+// this order: the densest groups first, the same cut into launches of
+// 65,536 / 16,384 (a barrier between launches drains the retry chains of hot
+// rows, as the reference's batch loop does), then fewer transactions in
+// flight, then more.
+const int kArms[][4] = {{5, 32, 1, 0}, {5, 32, 2, 0}, {5, 32, 1, 65536}, {5, 32, 2, 16384},
+                        {5, 32, 4, 0}, {4, 32, 2, 0}, {5, 16, 1, 0}, {4, 32, 1, 0},
+                        {3, 32, 2, 0}, {3, 32, 1, 0}};
 
 // Batch class: log2 of the batch size and the mean requests per tx in
 // steps of 8.
@@ -938,7 +947,7 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
     const int s = gcc_scheme_id(rp->cc_scheme);
     if (s < 0 || !var_scheme(s)) return GCC_EINVAL;
     if (mode != GCC_BATCHES_SEQUENTIAL && mode != GCC_BATCHES_QUEUE) return GCC_EINVAL;
-    if (mode == GCC_BATCHES_QUEUE && s == S_MVCC) return GCC_EINVAL;
+    if (mode == GCC_BATCHES_QUEUE && is_mvcc(s)) return GCC_EINVAL;
     if (rp->warp_density < 2 || rp->warp_density > 5) return GCC_EINVAL;
     if (rp->block_size < 1 || rp->block_size > 32) return GCC_EINVAL;
     if (rp->write_mode != GCC_WRITE_FIELD) return GCC_EINVAL;
@@ -958,6 +967,7 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
     if (rp->max_active < 0 || rp->starve_limit < -1) return GCC_EINVAL;
     std::vector<int> wd(nconf, rp->warp_density), bs(nconf, rp->block_size), cls(nconf, -1);
     std::vector<int> dv(nconf, 1);
+    std::vector<uint32_t> split(nconf, 0);
     if (autotune) {
         for (uint64_t b = 0; b < nconf; ++b) {
             cls[b] = mode == GCC_BATCHES_QUEUE ? -1 : batch_class(e->tx_off_h, batch_off[b], batch_off[b + 1]);
@@ -968,7 +978,8 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
                     const uint64_t full =
                         (uint64_t)std::max(0, occupancy_var(s, G, block)) * e->sm_count;
                     const uint64_t act = std::max<uint64_t>(1, full / a[2]) * (uint64_t)(block / G);
-                    arms.push_back({a[0], a[1], a[2], act, 0.0, 0});
+                    if (mode == GCC_BATCHES_QUEUE && a[3]) continue;  // one launch in queue mode
+                    arms.push_back({a[0], a[1], a[2], (uint32_t)a[3], act, 0.0, 0});
                 }
         }
         // one untried arm per class per run, so the runs of a class measure
@@ -980,11 +991,17 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
             wd[b] = it->second->wd;
             bs[b] = it->second->bs;
             dv[b] = it->second->div;
+            split[b] = it->second->split;
         }
     }
     uint64_t max_batch = 0;
     for (uint64_t b = 0; b < nb; ++b) max_batch = std::max<uint64_t>(max_batch, batch_off[b + 1] - batch_off[b]);
-    if (s == S_MVCC && e->ver_units * kMaxOps < max_batch * kMaxVarOps) {
+    if (is_slow(s) && !e->latch) {
+        if ((rc = e->alloc(&e->latch, e->rows * 4))) return rc;
+        cudaError_t le = cudaMemsetAsync(e->latch, 0, e->rows * 4, e->stream);
+        if (le != cudaSuccess) return e->fail_cuda(le);
+    }
+    if (is_mvcc(s) && e->ver_units * kMaxOps < max_batch * kMaxVarOps) {
         uint64_t nodes = max_batch * kMaxVarOps;
         if ((rc = e->alloc(&e->ver_ts, nodes * 8))) return rc;
         if ((rc = e->alloc(&e->ver_prev, nodes * 4))) return rc;
@@ -1030,8 +1047,21 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
     std::vector<uint64_t> key = {(uint64_t)s, (uint64_t)mode, rp->flags, rp->write_seed,
                                  p.spin_limit_ns, p.backoff_ns, p.starve_limit, (uint64_t)e->n_var, nb};
     for (uint64_t b = 0; b <= nb; ++b) key.push_back(batch_off[b]);
-    for (uint64_t b = 0; b < nconf; ++b)
+    for (uint64_t b = 0; b < nconf; ++b) {
         key.push_back(((uint64_t)wd[b] << 48) | ((uint64_t)bs[b] << 32) | (uint64_t)grid[b]);
+        key.push_back(split[b]);
+    }
+    // transaction-kernel launches of the run
+    uint64_t launches = 0;
+    if (mode == GCC_BATCHES_QUEUE) {
+        launches = 1;
+    } else {
+        for (uint64_t b = 0; b < nb; ++b) {
+            const uint64_t n = batch_off[b + 1] - batch_off[b];
+            const uint64_t step = split[b] ? std::min<uint64_t>(split[b], n) : n;
+            launches += (n + step - 1) / step;
+        }
+    }
 
     cudaStream_t st = e->stream;
     unsigned long long *stamp = e->stamps;
@@ -1039,8 +1069,7 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
         k_stamp<<<1, 1, 0, st>>>(stamp, i);
         return cudaGetLastError();
     };
-    const bool needs_reset = s == S_TO || s == S_MVCC ||
-                             !(rp->flags & GCC_F_NO_RESET);
+    const bool needs_reset = uses_ts(s) || !(rp->flags & GCC_F_NO_RESET);
     auto enqueue = [&]() -> cudaError_t {
         cudaError_t ce = cudaMemsetAsync(e->ctr, 0, sizeof(Counters), st);
         if (ce == cudaSuccess) ce = mark(0);
@@ -1049,7 +1078,7 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
             // launch that drains positions 0..n_var-1 in order
             if (ce == cudaSuccess) ce = cudaMemsetAsync(e->meta, 0, e->rows * 8, st);
             if (ce == cudaSuccess) {
-                k_batch_prep<<<1, 32, 0, st>>>(e->ctr, s == S_TO ? 1 : 0);
+                k_batch_prep<<<1, 32, 0, st>>>(e->ctr, uses_ts(s) ? 1 : 0);
                 k_set_u64<<<1, 1, 0, st>>>(e->queue_tail, e->n_var);
                 ce = cudaGetLastError();
             }
@@ -1068,13 +1097,27 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
                 ce = mark(3 + 3 * (int)b);
                 if (ce == cudaSuccess && (needs_reset || b == 0))
                     ce = cudaMemsetAsync(e->meta, 0, e->rows * 8, st);
-                if (ce == cudaSuccess && s == S_MVCC) ce = cudaMemsetAsync(e->turn, 0xFF, e->rows * 4, st);
+                if (ce == cudaSuccess && is_mvcc(s)) ce = cudaMemsetAsync(e->turn, 0xFF, e->rows * 4, st);
                 if (ce == cudaSuccess) {
-                    k_batch_prep<<<1, 32, 0, st>>>(e->ctr, (s == S_TO || s == S_MVCC) ? 1 : 0);
+                    k_batch_prep<<<1, 32, 0, st>>>(e->ctr, uses_ts(s) ? 1 : 0);
                     ce = cudaGetLastError();
                 }
                 if (ce == cudaSuccess) ce = mark(4 + 3 * (int)b);
-                if (ce == cudaSuccess) ce = launch_var(s, 1 << wd[b], grid[b], block[b], q, st);
+                // the batch in launches of at most split[b] transactions
+                // (the tickets restart per launch; timestamps and metadata
+                // carry on inside the batch)
+                const uint32_t bn = q.batch_n;
+                const uint32_t step = split[b] ? std::min<uint32_t>(split[b], bn) : bn;
+                for (uint32_t o = 0; o < bn && ce == cudaSuccess; o += step) {
+                    KParams r = q;
+                    r.batch_st = q.batch_st + o;
+                    r.batch_n = std::min<uint32_t>(step, bn - o);
+                    if (o) {
+                        k_batch_prep<<<1, 32, 0, st>>>(e->ctr, 0);
+                        ce = cudaGetLastError();
+                    }
+                    if (ce == cudaSuccess) ce = launch_var(s, 1 << wd[b], grid[b], block[b], r, st);
+                }
                 if (ce == cudaSuccess) ce = mark(5 + 3 * (int)b);
             }
         }
@@ -1124,6 +1167,7 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
     e->bstat_bs.assign(nconf, 0);
     e->bstat_ms.assign(nconf, 0.0);
     e->bstat_active.assign(nconf, 0);
+    e->bstat_split.assign(nconf, 0);
     for (uint64_t b = 0; b < nconf; ++b) {
         double kms;
         if (mode == GCC_BATCHES_QUEUE) {
@@ -1137,6 +1181,7 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
         e->bstat_bs[b] = bs[b];
         e->bstat_ms[b] = kms;
         e->bstat_active[b] = (uint64_t)grid[b] * (uint64_t)(block[b] >> wd[b]);
+        e->bstat_split[b] = split[b];
     }
     const double tot_ms = span_ms(0, 2);
     if (autotune && !hc.err) {
@@ -1154,7 +1199,8 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
                 if (a.wd != wd[0] && mode == GCC_BATCHES_QUEUE) continue;
                 bool match = false;
                 for (uint64_t b = 0; b < nconf; ++b)
-                    if (cls[b] == kv.first && wd[b] == a.wd && bs[b] == a.bs && dv[b] == a.div)
+                    if (cls[b] == kv.first && wd[b] == a.wd && bs[b] == a.bs && dv[b] == a.div &&
+                        split[b] == a.split)
                         match = true;
                 if (!match) continue;
                 double v = kv.second.first / (double)kv.second.second;
@@ -1179,13 +1225,20 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
     out->tot_d = hc.tot_cycles * inv;
     out->idx_d = hc.idx_cycles * inv;
     out->batches = nb;
-    out->kernel_launches = mode == GCC_BATCHES_QUEUE ? 3 : 2 * nb;
+    // transaction kernels + per-batch prep (+ the queue tail write)
+    out->kernel_launches = mode == GCC_BATCHES_QUEUE ? launches + 2 : 2 * launches;
     out->max_attempts = hc.max_attempts;
     out->err_site = hc.err_where;
     out->lat_p50_us = hist_percentile_us(hc, 0.50);
     out->lat_p99_us = hist_percentile_us(hc, 0.99);
     if (hc.err) return (int)hc.err;
     if (hc.committed != e->n_var) return GCC_ESTATE;
+    return GCC_OK;
+}
+
+int gcc_get_batch_split(gcc_engine *e, uint32_t *split, uint64_t n) {
+    if (!e || !split || n > e->bstat_split.size()) return GCC_EINVAL;
+    std::copy(e->bstat_split.begin(), e->bstat_split.begin() + n, split);
     return GCC_OK;
 }
 

@@ -321,15 +321,19 @@ int gcc_load_var_txs(gcc_engine *e, const uint32_t *tx_off, const gcc_ycsb_req *
                                     no per-batch barrier (tpl_nw, tpl_wd, to,
                                     silo, tictoc) */
 /* Extra run flags of gcc_run_batches. */
-#define GCC_F_AUTOTUNE 16u /* choose warp_density / block_size per batch class
-                              (size, requests per tx) from measured runs */
+#define GCC_F_AUTOTUNE 16u /* choose warp_density / block_size / transactions
+                              in flight / batch_size per batch class (size,
+                              requests per tx) from measured runs */
 #define GCC_F_GRAPH 32u    /* capture the whole run in a CUDA graph once and
                               replay it while the configuration is unchanged */
 
 /* Run the loaded variable-length transactions split into n_batches batches
- * (batch b = transactions batch_off[b] .. batch_off[b+1]). Schemes: tpl_nw,
- * tpl_wd, to, silo, tictoc, mvcc (sequential only); warp_density 2..5.
- * Synchronous. */
+ * (batch b = transactions batch_off[b] .. batch_off[b+1]). Schemes: every
+ * scheme but gacco and gputx (their ordering passes take 16-request records),
+ * mvcc and slow_mvcc in sequential mode only; warp_density 2..5. With
+ * GCC_F_AUTOTUNE the tuner picks per batch class warp_density, block_size,
+ * the transactions in flight and the batch_size of the launches inside a
+ * batch. Synchronous. */
 int gcc_run_batches(gcc_engine *e, const gcc_run_params *p, const uint32_t *batch_off,
                     uint64_t n_batches, int32_t mode, gcc_result *out);
 
@@ -342,6 +346,12 @@ int gcc_get_batch_stats(gcc_engine *e, int32_t *warp_density, int32_t *block_siz
  * entry of the last gcc_run_batches, entry for entry as gcc_get_batch_stats.
  * No counterpart in the reference (its grid covers the whole batch). */
 int gcc_get_batch_active(gcc_engine *e, uint64_t *active, uint64_t n);
+
+/* batch_size the autotuner chose for each batch of the last gcc_run_batches
+ * (entry for entry as gcc_get_batch_stats): the batch ran in launches of at
+ * most this many transactions, 0 = one launch for the whole batch (the
+ * reference's batch_size knob, benchmark_cpu/ycsb.cu:262-271). */
+int gcc_get_batch_split(gcc_engine *e, uint32_t *split, uint64_t n);
 
 /* Results of the last run / current state (device -> host copies). */
 int gcc_dump_table(gcc_engine *e, void *host_dst, uint64_t bytes); /* packed rows */

@@ -200,3 +200,34 @@ def write_field(write_seed, tx, op):
 def write_value(write_seed, tx, op):
     """Value that write request `op` of transaction `tx` stores."""
     return _h3(write_seed, tx, 2 * op + 1)
+
+
+def gputx_rank_hazards(txs, rows):
+    """Where the reference's GPUTx run is not deterministic on `txs`, so
+    that its output cannot be compared byte for byte: (same_rank_conflicts,
+    last_object_accesses).
+      same_rank_conflicts: (row, rank) groups that two or more transactions
+        of the same rank access with at least one write; the reference runs
+        a rank in one launch without ordering them (src/gputx.cu:17-27,
+        include/gputx.cuh:289-294);
+      last_object_accesses: accesses to the highest accessed row; the
+        reference's rank pass reads that row's list end one past its scanned
+        offsets (offset[dense_cnt], include/gputx.cuh:252-253 and
+        src/gputx.cu:17-18), so only a row accessed once ranks the same."""
+    ranks, _, _ = gputx_order(txs, rows)
+    cnt = txs["request_cnt"].astype(np.int64)
+    valid = np.arange(16)[None, :] < cnt[:, None]
+    t = np.broadcast_to(np.arange(len(txs))[:, None], valid.shape)[valid]
+    k = txs["requests"]["key"].astype(np.int64)[valid]
+    w = (txs["requests"]["read"] == 0)[valid]
+    r = np.asarray(ranks, dtype=np.int64)[t]
+    o = np.lexsort((t, r, k))
+    k, r, w = k[o], r[o], w[o]
+    start = np.ones(len(k), dtype=bool)
+    start[1:] = (k[1:] != k[:-1]) | (r[1:] != r[:-1])
+    gid = np.cumsum(start) - 1
+    size = np.bincount(gid)
+    anyw = np.bincount(gid, weights=w.astype(np.float64)) > 0
+    same_rank = int(((size >= 2) & anyw).sum())
+    last = int((k == k.max()).sum()) if len(k) else 0
+    return same_rank, last

@@ -42,7 +42,7 @@ def check(oracle, eng, init, off, reqs, seed):
 @pytest.mark.parametrize("wd", [5, 3])
 def test_batches_parity(oracle, var_setup, scheme, mode, wd):
     eng, init, off, reqs = var_setup
-    if mode == g.BATCHES_QUEUE and scheme == "mvcc":
+    if mode == g.BATCHES_QUEUE and scheme in ("mvcc", "slow_mvcc"):
         with pytest.raises(g.GccError):
             eng.run_batches(scheme, BATCHES, mode, warp_density=wd, block_size=8)
         return
@@ -83,3 +83,30 @@ def test_batches_reject_bad_arguments(var_setup):
         eng.run_batches("tpl_nw", np.array([0, 10], dtype=np.uint32))  # must cover all txs
     with pytest.raises(g.GccError):
         eng.run_batches("tpl_nw", BATCHES, warp_density=1)
+
+
+def test_autotuner_batch_size_arms(oracle):
+    """The tuner's arms include batch_size (launches of at most 16,384 /
+    65,536 transactions inside a batch); a batch cut into launches still
+    replays bit-exactly."""
+    rows = 200000
+    off, reqs = g.gen_ycsb_var(rows, 40000, 0.6, 0.8, min_ops=4, max_ops=32, seed=23)
+    init = oracle.fill_table(rows, g.LAYOUT_U64X11, 3)
+    boff = np.array([0, 20000, 40000], dtype=np.uint32)
+    splits = set()
+    with g.Engine(rows, layout=g.LAYOUT_U64X11, index=g.INDEX_HASH, fill_seed=3,
+                  max_batch=20000) as eng:
+        eng.load_var_txs(off, reqs)
+        for run in range(11):
+            eng.upload_table(init)
+            res = eng.run_batches("tpl_nw", boff, g.BATCHES_SEQUENTIAL, warp_density=5,
+                                  block_size=32, flags=g.F_COMMIT_LOG | g.F_AUTOTUNE,
+                                  write_seed=9, spin_limit_ns=SPIN)
+            assert res["committed"] == len(off) - 1
+            check(oracle, eng, init, off, reqs, 9)
+            sp = eng.batch_split()
+            assert set(sp.tolist()) <= {0, 16384, 65536}
+            splits.update(sp.tolist())
+            if 16384 in sp.tolist():
+                assert res["kernel_launches"] >= 2 * 3  # 2 launches for a 20,000 batch
+    assert 16384 in splits or 65536 in splits

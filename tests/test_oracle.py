@@ -119,3 +119,54 @@ def test_golden_fixtures(oracle):
         import hashlib
         assert hashlib.sha256(t.tobytes()).hexdigest() == case["table_sha256"], case["name"]
         assert hashlib.sha256(dg.tobytes()).hexdigest() == case["digests_sha256"], case["name"]
+
+
+@pytest.mark.parametrize("args", [(100_000, 4000, 0.6, 0.9, 141919810, 1, 0),
+                                  (4096, 3000, 0.99, 0.5, 5, 0, 1),
+                                  (1_000_000, 2000, 0.1, 1.0, 7, 0, 1)])
+def test_oracle_generator_equals_engine_generator(oracle, args):
+    """The bench's reference arms take their records from the oracle's
+    generator and the engine's arm from its own: they must be the same."""
+    rows, n, theta, r, seed, dedup, kb = args
+    a = g.gen_ycsb(rows, n, theta, r, seed=seed, dedup=dedup, key_base=kb)
+    b = oracle.gen_ycsb(rows, n, theta, r, seed, dedup, kb)
+    assert np.array_equal(a.view(np.uint8), b.view(np.uint8))
+
+
+def test_oracle_write_formulas_match_replay(oracle):
+    """write_field / write_value (Python) against the C replay."""
+    rows, layout = 8, g.LAYOUT_U64X11
+    txs = np.zeros(3, dtype=g.TX_DTYPE)
+    for t in range(3):
+        txs[t]["request_cnt"] = 2
+        txs[t]["requests"][0] = (0, t + 1)
+        txs[t]["requests"][1] = (0, t + 4)
+    init = oracle.fill_table(rows, layout, 0)
+    t_out, _, _ = oracle.replay(init, layout, txs, np.arange(3, dtype=np.uint32), g.WRITE_FIELD, 77)
+    w = t_out.view(np.uint64).reshape(rows, 11)
+    for t in range(3):
+        for i, row in enumerate((t + 1, t + 4)):
+            f = oracle.write_field(77, t, i)
+            assert int(w[row, 1 + f]) == oracle.write_value(77, t, i)
+
+
+def test_gputx_rank_hazards_known_answer(oracle):
+    """Two transactions that write the same row get ranks 0 and 1 (no
+    hazard); adding a third that makes a same-rank write pair is one."""
+    rows = 16
+    txs = np.zeros(2, dtype=g.TX_DTYPE)
+    txs[0]["request_cnt"] = 1
+    txs[0]["requests"][0] = (0, 3)
+    txs[1]["request_cnt"] = 2
+    txs[1]["requests"][0] = (0, 3)
+    txs[1]["requests"][1] = (1, 9)
+    assert oracle.gputx_rank_hazards(txs, rows) == (0, 1)
+    # tx2 reads row 5 (rank 0 there) and writes row 9 after tx1's read
+    # (rank 1 there): rank 1 equals tx1's, and both touch row 9 with a write
+    t3 = np.zeros(3, dtype=g.TX_DTYPE)
+    t3[:2] = txs
+    t3[2]["request_cnt"] = 2
+    t3[2]["requests"][0] = (1, 5)
+    t3[2]["requests"][1] = (0, 9)
+    sr, last = oracle.gputx_rank_hazards(t3, rows)
+    assert sr == 1 and last == 2
