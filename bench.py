@@ -88,10 +88,12 @@ def parse():
                     help="comma list of extra schemes timed once on the same workload "
                          "('' for none)")
     ap.add_argument("--workload", default="plain",
-                    choices=["plain", "batched", "learned", "serving"],
+                    choices=["plain", "batched", "learned", "serving", "sweep"],
                     help="plain: 1,048,576 x 16-request transactions in 65,536 batches; "
                          "batched: 64 uneven batches of 4-64-request transactions; "
                          "learned: 256 drifting-contention batches, learned scheduling")
+    ap.add_argument("--sweep-txs", type=int, default=262_144,
+                    help="transactions per point of the sweep workload's scheme grid")
     ap.add_argument("--batches", type=int, default=None,
                     help="batches of the batched (64) / learned (256) workloads")
     a = ap.parse_args()
@@ -741,6 +743,120 @@ def run_serving(a):
         dist.destroy_process_group()
 
 
+def run_sweep(a):
+    """The plain-YCSB scheme sweep on one B200 (BASELINE's second
+    configuration): every scheme x theta {0.1, 0.6, 0.8, 0.99} x read ratio
+    {1.0, 0.9, 0.5} at warp_density 5 / block_size 32, and the warp_density
+    0-5 x block_size {1, 8, 16, 32} grid at theta 0.6 and 0.99 (tpl_nw and
+    silo), on 10,485,760 rows with --txs transactions of 16 requests in
+    batches of --batch; per point committed tx/s (the reference's tot_time
+    definition), aborted attempts and algorithmic GB/s of the transaction
+    kernel. Then the reference's own dataset points in its own format
+    (104 B rows, sorted index, whole-row copies, batch 1,048,576): ro (theta
+    0, reads only), mc (theta 0.6, r 0.9), hc (theta 0.8, r 0.5) and t9
+    (theta 0.9, r 0.9, the highest contention the reference publishes), for
+    the engine and for the reference's GPU build (not at theta 0.99: its
+    retries are immediate and unbounded, and its published runs stop at
+    0.9). One JSON line per point, then the summary line. The scheme grid
+    uses --sweep-txs transactions per point, the reference points --txs."""
+    from gpu_cc_tb_b200 import replicas
+    rank, ws, local, dist = replicas.init_from_env("nccl")
+    import gpu_cc_tb_b200 as g
+    hbm, kind = peaks()
+    clocks = Clocks(local)
+    clocks.start()
+    points = []
+
+    def point(eng, txs, alg, s, theta, r, wd, bs, extra=None):
+        k = dict(warp_density=wd, block_size=bs, batch_size=a.batch, write_seed=1)
+        if s in QUEUE_DEFAULT and not a.no_queue:
+            k["flags"] = g.F_QUEUE
+        try:
+            eng.run(s, **k)
+            res = eng.run(s, **k)
+            km, _ = eng.last_kernel_ms()
+            pt = {"scheme": s, "theta": theta, "read_ratio": r, "wd": wd, "bs": bs,
+                  "tx_per_s": res["tx_per_s"], "aborts": res["aborts"],
+                  "alg_gbs": alg / (km / 1e3) / 1e9 if km > 0 else None,
+                  "p99_us": res["lat_p99_us"], "queue": bool(k.get("flags", 0))}
+        except g.GccError as e:
+            pt = {"scheme": s, "theta": theta, "read_ratio": r, "wd": wd, "bs": bs,
+                  "error": str(e)}
+        if extra:
+            pt.update(extra)
+        points.append(pt)
+        if rank == 0:
+            print(json.dumps(pt), flush=True)
+
+    with g.Engine(a.rows, layout=g.LAYOUT_U64X11, index=g.INDEX_HASH, fill_seed=141919810,
+                  device=local, max_batch=a.batch) as eng:
+        for theta in (0.1, 0.6, 0.8, 0.99):
+            for r in (1.0, 0.9, 0.5):
+                txs = g.gen_ycsb(a.rows, a.sweep_txs, theta, r, seed=141919810,
+                                 dedup=g.DEDUP_RESAMPLE, key_base=0)
+                alg, _, _ = algorithmic_bytes(txs)
+                eng.load_txs(txs)
+                for s in g.SCHEMES:
+                    point(eng, txs, alg, s, theta, r, 5, 32)
+                if r == 0.9 and theta in (0.6, 0.99):
+                    for s in ("tpl_nw", "silo"):
+                        for wd in range(6):
+                            for bs in (1, 8, 16, 32):
+                                if (wd, bs) != (5, 32):
+                                    point(eng, txs, alg, s, theta, r, wd, bs, {"grid": True})
+    # the reference's dataset points, engine and reference build side by side
+    ref_points = {}
+    from oracle import ref_gpu
+    for name, theta, r in (("ro", 0.0, 1.0), ("mc", 0.6, 0.9), ("hc", 0.8, 0.5), ("t9", 0.9, 0.9)):
+        etx = g.gen_ycsb(a.rows, a.txs, theta, r, seed=141919810, dedup=g.DEDUP_DROP, key_base=1)
+        rp = {"engine": {}, "reference": {}}
+        with g.Engine(a.rows, layout=g.LAYOUT_REF104, index=g.INDEX_SORTED, fill_seed=0,
+                      device=local, max_batch=a.txs) as e:
+            e.load_txs(etx)
+            for s in g.SCHEMES:
+                k = dict(warp_density=5, block_size=32, batch_size=a.txs,
+                         write_mode=g.WRITE_ROWCOPY, write_seed=1)
+                try:
+                    e.run(s, **k)
+                    rp["engine"][s] = e.run(s, **k)["tx_per_s"]
+                except g.GccError as ex:
+                    rp["engine"][s] = str(ex)
+        if ref_gpu.available():
+            from oracle import oracle_py as o
+            rtx = o.gen_ycsb(a.rows, a.txs, theta, r, 141919810, 0, 1)
+            with tempfile.TemporaryDirectory() as td:
+                ds = Path(td) / f"{name}.txs"
+                ds.write_bytes(rtx.tobytes())
+                for s in g.SCHEMES:
+                    ok, why = ref_gpu.runnable(s, a.txs, 5, a.txs)
+                    if not ok:
+                        rp["reference"][s] = f"not run: {why}"
+                        continue
+                    try:
+                        rp["reference"][s] = ref_gpu.run(ds, a.rows, a.txs, s, 5, 32, a.txs,
+                                                         timeout=600)["through"]
+                    except Exception as ex:
+                        rp["reference"][s] = f"error: {str(ex)[-200:]}"
+        ref_points[name] = rp
+        if rank == 0:
+            print(json.dumps({"ref_point": name, **rp}), flush=True)
+    clk = clocks.stop()
+    if rank == 0:
+        best = {}
+        for pt in points:
+            if "tx_per_s" in pt and not pt.get("grid"):
+                best[f"{pt['scheme']}_t{pt['theta']}_r{pt['read_ratio']}"] = pt["tx_per_s"]
+        print(json.dumps({"metric": "committed tx/s", "workload": "plain YCSB scheme sweep",
+                          "unit": "tx/s", "rows": a.rows, "transactions": a.sweep_txs,
+                          "reference_point_transactions": a.txs,
+                          "batch_size": a.batch, "points": len(points), "by_point": best,
+                          "reference_points": ref_points, "hbm_peak_gbs": hbm,
+                          "peak_kind": kind, "clocks": clk}), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -754,6 +870,9 @@ def main():
         return
     if a.workload == "serving":
         run_serving(a)
+        return
+    if a.workload == "sweep":
+        run_sweep(a)
         return
     from gpu_cc_tb_b200 import replicas
     rank, ws, local, dist = replicas.init_from_env("nccl")

@@ -1171,10 +1171,17 @@ __host__ __device__ constexpr bool is_ordered(int s) { return s == S_GACCO || s 
 // at theta 0.6 and +25-50 % at 0.8-0.99; TO 22.9 -> 57 M tx/s at 0.6 and
 // unchanged at 0.8-0.99; tpl_nw 58 -> 67 M at 0.6, -5 % at 0.8, unchanged
 // at 0.9-0.99 (never ordering 2PL / TO gives 98 M at 0.6 but -35 % at 0.8
-// and above). The latch variants go ordered from the first retry.
+// and above). The latch variants follow their fast counterparts (ordering
+// them from the first retry made every retry 16 dependent latch round trips
+// and left slow_tpl_nw at a tenth of tpl_nw at theta 0.6); MVCC and the
+// ordered schemes keep requests in program order.
 __host__ __device__ constexpr unsigned ordered_after(int s) {
-    return (s == S_SILO || s == S_TICTOC) ? 0xFFFFFFFFu
-                                          : ((s == S_TO || s == S_TPL_NW || s == S_TPL_WD) ? 16u : 1u);
+    return (s == S_SILO || s == S_TICTOC || s == S_SLOW_SILO || s == S_SLOW_TICTOC)
+               ? 0xFFFFFFFFu
+               : ((s == S_TO || s == S_TPL_NW || s == S_TPL_WD || s == S_SLOW_TO ||
+                   s == S_SLOW_TPL_NW || s == S_SLOW_TPL_WD)
+                      ? 16u
+                      : 1u);
 }
 
 // ===========================================================================
