@@ -340,36 +340,83 @@ def learned_vs_plain(g, eng, a, sch, n_batches=16, theta=0.99):
 
 
 def run_reference(a):
-    """--impl reference: the CPU port of the path on the host cores. It uses
-    nothing of the engine: inputs come from the oracle's own generator (the
-    same records as the engine's for the same seed)."""
+    """--impl reference: the reference's own implementation of the path,
+    timed on this machine. The reference has no CPU execution path (its
+    benchmark_cpu/ycsb.cu is the host driver that NVRTC-compiles and
+    launches its GPU kernel), so this is its own test_ycsb, compiled from its
+    sources into oracle/_ref/ (oracle/Makefile), run unmodified on the
+    workload's shape: the same rows, transactions, theta, read ratio, scheme,
+    batch_size, warp_density and block_size, in its own record semantics
+    (repeated keys dropped, keys 1..rows-1) and row format (104-byte Item
+    rows, whole-row copies on write, sorted-array index) -- the only format
+    it has. Each step is one test_ycsb run; the value is committed
+    transactions over its own tot_time (metadata resets + precompute +
+    kernels, benchmark_cpu/ycsb.cu:249-291). The line also carries the
+    project's CPU port of the CC rules on all host threads (`cpu_port`).
+    It uses nothing of the engine: records come from the oracle's
+    generator."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from oracle import oracle_py as o
-    txs = o.gen_ycsb(a.rows, a.txs, a.theta, a.read_ratio, 141919810, 1, 0)  # dedup resample
+    from oracle import ref_gpu
     threads = a.cpu_threads or os.cpu_count()
-    sch = a.scheme if a.scheme in ("tpl_nw", "silo", "tictoc") else "tpl_nw"
-    n = len(txs)
-    init = o.fill_table(a.rows, 0, 141919810)
-    times = []
-    for step in range(a.warmup + a.steps):
-        sample = txs[(step * n) % len(txs):][:n]
-        _, _, _, secs, _ = o.cpu_run(sch, init, 0, sample, 0, 1, threads=threads,  # field writes
-                                     commit_log=False)
-        if step >= a.warmup:
-            times.append(secs)
-    tot = sum(times)
-    v = a.steps * n / tot
+    sch = a.scheme
     cfg = config_of(a)
-    cfg["cc_scheme"] = sch
+    cfg.update({"layout": "reference Item rows (uint32 id + 10 x char[10] = 104 B)",
+                "write": "whole-row copy of the last row read (benchmark/ycsb.cu:57-98)",
+                "index": "sorted array (include/index.cuh:65-92)",
+                "records": "repeated keys dropped, keys in [1, rows-1] (generation/gen_ycsb.cu)",
+                "execution": "the reference's batch loop, one launch per batch"})
+    # the project's CPU port of the CC rules, on the engine line's records
+    ctx = o.gen_ycsb(a.rows, a.txs, a.theta, a.read_ratio, 141919810, 1, 0)  # dedup resample
+    csch = sch if sch in ("tpl_nw", "silo", "tictoc") else "tpl_nw"
+    init = o.fill_table(a.rows, 0, 141919810)
+    _, _, _, csecs, _ = o.cpu_run(csch, init, 0, ctx, 0, 1, threads=threads, commit_log=False)
+    cpu_port = {"value": len(ctx) / csecs, "unit": "tx/s", "cores": threads, "kind": "port",
+                "scheme": csch,
+                "sample": f"all {len(ctx)} transactions, one pass, {threads} threads, {a.rows} rows"}
+    ok, why = ref_gpu.runnable(sch, a.txs, a.wd, a.batch)
+    if not ref_gpu.available() or not ok:
+        reason = why or "the reference build is missing (make -C oracle ref REF=<dir>)"
+        print(json.dumps({"impl": "reference", "unavailable": reason, "cpu_port": cpu_port}),
+              flush=True)
+        return
+    rtx = o.gen_ycsb(a.rows, a.txs, a.theta, a.read_ratio, 141919810, 0, 1)  # dedup drop
+    times, walls, aborts = [], [], []
+    with tempfile.TemporaryDirectory() as td:
+        ds = Path(td) / "ycsb.txs"
+        ds.write_bytes(rtx.tobytes())
+        try:
+            for step in range(a.warmup + a.steps):
+                r = ref_gpu.run(ds, a.rows, len(rtx), sch, a.wd, a.bs, a.batch, timeout=600)
+                if step >= a.warmup:
+                    times.append(r["tot"])
+                    walls.append(r["wall_s"])
+                    aborts.append(r.get("abort", 0))
+        except (RuntimeError, OSError, subprocess.TimeoutExpired) as e:
+            # e.g. no GPU on this machine: the reference cannot run at all
+            print(json.dumps({"impl": "reference",
+                              "unavailable": "the reference's test_ycsb did not run: "
+                                             + str(e).splitlines()[0][:200],
+                              "cpu_port": cpu_port}), flush=True)
+            return
+    tot = sum(times)
+    v = a.steps * len(rtx) / tot
     line = {"impl": "reference", "metric": "committed tx/s", "value": v, "unit": "tx/s",
-            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+            "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": 1000 * tot / a.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded gen_ycsb)",
+            "vs_baseline": None, "dtype": "u32 keys / byte rows", "data": "synthetic (seeded gen_ycsb semantics)",
             "config": cfg,
-            "cpu_baseline": {"value": v, "unit": "tx/s", "cores": threads, "kind": "port",
-                             "sample": f"{n} transactions per step, {threads} threads"},
+            "program": "reference test_ycsb, unmodified (oracle/_ref), its NVRTC kernel "
+                       "JIT-compiled for sm_100 by the CUDA driver",
+            "aborts_per_step": statistics.mean(aborts),
+            "wall_s_per_step": statistics.mean(walls),
+            "cpu_baseline": {"value": v, "unit": "tx/s", "cores": 1, "kind": "reference",
+                             "sample": f"{len(rtx)} transactions per step; the reference's "
+                                       "host driver is one thread and runs its kernel on "
+                                       "the GPU (it has no CPU path)"},
+            "cpu_port": cpu_port,
             "e2e": {"value": v, "unit": "tx/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
