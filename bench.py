@@ -293,7 +293,7 @@ def engine_reference_format(g, a, txs, local, index_kind):
     return out
 
 
-CAPS = (256, 512, 1024, 2048)
+CAPS = (128, 256, 512, 1024, 2048)
 
 
 def learned_vs_plain(g, eng, a, sch, n_batches=16, theta=0.99):
@@ -305,10 +305,12 @@ def learned_vs_plain(g, eng, a, sch, n_batches=16, theta=0.99):
       plain_best   the plain kernel at its best in-flight cap (max_active
                    swept over CAPS) -- the honest denominator;
       learned      the learned scheduler (predictor trained online, the
-                   measured policy, deferral and caps) after two training
-                   passes;
+                   measured policy, deferral and caps, 2PL lock plans from
+                   its key-frequency table) after two training passes;
       untrained    the same scheduler with the network left at its initial
-                   weights (train_steps -1): the ablation of the network."""
+                   weights (train_steps -1): the ablation of the network;
+      no_plan      the same scheduler without lock plans (plan_threshold
+                   -1): the ablation of the frequency-table lock order."""
     txs = g.gen_ycsb(a.rows, n_batches * a.batch, theta, a.read_ratio, seed=20240521,
                      dedup=g.DEDUP_RESAMPLE, key_base=0)
     eng.load_txs(txs)
@@ -325,8 +327,9 @@ def learned_vs_plain(g, eng, a, sch, n_batches=16, theta=0.99):
     best = max(caps, key=caps.get)
     out["plain_caps"] = caps
     out["plain_best"] = {"max_active": best, "tx_per_s": caps[best]}
-    for name, steps in (("learned", 0), ("untrained", -1)):
-        with g.Scheduler(eng, mode=g.SCHED_LEARNED, train_steps=steps, seed=7) as sc:
+    for name, steps, plan in (("learned", 0, 0), ("untrained", -1, 0), ("no_plan", 0, -1)):
+        with g.Scheduler(eng, mode=g.SCHED_LEARNED, train_steps=steps, seed=7,
+                         plan_threshold=plan) as sc:
             sc.run(sch, **kw)
             sc.run(sch, **kw)
             r = sc.run(sch, **kw)
@@ -336,6 +339,7 @@ def learned_vs_plain(g, eng, a, sch, n_batches=16, theta=0.99):
     out["learned_over_plain"] = out["learned"]["tx_per_s"] / out["plain"]["tx_per_s"]
     out["learned_over_plain_best"] = out["learned"]["tx_per_s"] / out["plain_best"]["tx_per_s"]
     out["learned_over_untrained"] = out["learned"]["tx_per_s"] / out["untrained"]["tx_per_s"]
+    out["learned_over_no_plan"] = out["learned"]["tx_per_s"] / out["no_plan"]["tx_per_s"]
     return out
 
 

@@ -40,6 +40,7 @@ WRITE_FIELD, WRITE_ROWCOPY = 0, 1
 F_COMMIT_LOG, F_READ_LOG, F_NO_RESET, F_RETRY_IMMEDIATE = 1, 2, 4, 8
 F_AUTOTUNE, F_GRAPH = 16, 32
 F_QUEUE = 128  # gcc_run / gcc_run_host: all batches through one device-queue launch
+F_REQUEST_ORDER = 256  # 2PL / TO one-at-a-time retries in request order (the reference's)
 QUEUE_SCHEMES = ("tpl_nw", "tpl_wd", "to", "silo", "tictoc", "slow_tpl_nw", "slow_tpl_wd",
                  "slow_to", "slow_silo", "slow_tictoc")
 BATCHES_SEQUENTIAL, BATCHES_QUEUE = 0, 1
@@ -77,7 +78,8 @@ class RunParams(C.Structure):
                 ("block_size", C.c_int32), ("batch_size", C.c_int32), ("flags", C.c_uint32),
                 ("write_mode", C.c_int32), ("backoff_ns", C.c_int32), ("write_seed", C.c_uint64),
                 ("spin_limit_ns", C.c_uint64),
-                ("starve_limit", C.c_int32), ("max_active", C.c_int32)]
+                ("starve_limit", C.c_int32), ("max_active", C.c_int32),
+                ("ordered_after", C.c_int32), ("reserved", C.c_int32)]
 
 
 class Result(C.Structure):
@@ -105,7 +107,8 @@ class SchedParams(C.Structure):
     _fields_ = [("mode", C.c_int32), ("explore_every", C.c_int32), ("probe_rows", C.c_int32),
                 ("train_steps", C.c_int32), ("minibatch", C.c_int32), ("lr", C.c_float),
                 ("defer_threshold", C.c_float), ("fixed_arm", C.c_int32), ("min_sched", C.c_int32),
-                ("reserved", C.c_int32), ("seed", C.c_uint64)]
+                ("plan_threshold", C.c_int32), ("seed", C.c_uint64), ("plan_after", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class SchedBatch(C.Structure):
@@ -237,6 +240,7 @@ def library() -> C.CDLL:
         "gcc_sched_run": (C.c_int, [P, C.POINTER(RunParams), C.POINTER(SchedResult)]),
         "gcc_sched_batches": (C.c_int, [P, P, C.c_uint64]),
         "gcc_sched_features": (C.c_int, [P, C.c_uint64, C.c_uint64, P]),
+        "gcc_sched_lock_plans": (C.c_int, [P, C.c_uint64, C.c_uint64, P]),
         "gcc_sched_observe": (C.c_int, [P, C.c_uint64, C.c_uint64, C.c_int32]),
         "gcc_sched_features_var": (C.c_int, [P, C.c_uint64, C.c_uint64, P]),
         "gcc_sched_observe_var": (C.c_int, [P, C.c_uint64, C.c_uint64, C.c_int32]),
@@ -359,10 +363,11 @@ class Engine:
     def params(self, scheme: str, warp_density: int = 5, block_size: int = 32,
                batch_size: int = 65536, flags: int = 0, write_mode: int = WRITE_FIELD,
                write_seed: int = 1, spin_limit_ns: int = 0, backoff_ns: int = 0,
-               starve_limit: int = 0, max_active: int = 0) -> RunParams:
+               starve_limit: int = 0, max_active: int = 0, ordered_after: int = 0) -> RunParams:
         self._scheme = scheme.encode()
         return RunParams(self._scheme, warp_density, block_size, batch_size, flags, write_mode,
-                         backoff_ns, write_seed, spin_limit_ns, starve_limit, max_active)
+                         backoff_ns, write_seed, spin_limit_ns, starve_limit, max_active,
+                         ordered_after, 0)
 
     def run(self, scheme: str, **kw) -> dict:
         p = self.params(scheme, **kw)
@@ -498,12 +503,13 @@ class Scheduler:
     def __init__(self, engine: "Engine", mode: int = SCHED_LEARNED, explore_every: int = 0,
                  probe_rows: int = 0, train_steps: int = 0, minibatch: int = 0, lr: float = 0.0,
                  defer_threshold: float = 0.0, fixed_arm: int = 0, min_sched: int = 0,
-                 seed: int = 1):
+                 seed: int = 1, plan_threshold: int = 0, plan_after: int = 0):
         self.engine = engine
         self.lib = engine.lib
         self._h = C.c_void_p()
         prm = SchedParams(mode, explore_every, probe_rows, train_steps, minibatch, lr,
-                          defer_threshold, fixed_arm, min_sched, 0, seed)
+                          defer_threshold, fixed_arm, min_sched, plan_threshold, seed,
+                          plan_after, 0)
         _check(self.lib.gcc_sched_create(engine._h, C.byref(prm), C.byref(self._h)),
                "gcc_sched_create")
         self.n_params = int(self.lib.gcc_sched_param_count())
@@ -556,6 +562,13 @@ class Scheduler:
     def features(self, first: int, n: int) -> np.ndarray:
         out = np.zeros((n, SCHED_FEAT_STRIDE), dtype=np.uint16)
         _check(self.lib.gcc_sched_features(self._h, first, n, _ptr(out)), "gcc_sched_features")
+        return out
+
+    def lock_plans(self, first: int, n: int) -> np.ndarray:
+        """2PL lock plans (u64 per record) of records first .. first+n-1
+        against the current frequency table (gcc_sched_lock_plans)."""
+        out = np.zeros(n, dtype=np.uint64)
+        _check(self.lib.gcc_sched_lock_plans(self._h, first, n, _ptr(out)), "gcc_sched_lock_plans")
         return out
 
     def features_var(self, first: int, n: int) -> np.ndarray:

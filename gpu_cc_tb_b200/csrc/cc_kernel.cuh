@@ -100,6 +100,10 @@ struct TxOps {
     uint32_t isread;           // bit k: op k reads
     unsigned long long readmask;  // group-wide: bit i set if op i reads
     uint32_t row[K];
+    // 1 + the request that failed in the last aborted 2PL / TO attempt (0:
+    // none); the next one-at-a-time attempt visits it after the others
+    // (unless GCC_F_REQUEST_ORDER)
+    mutable uint32_t obst_op;
 };
 
 // Bounded wait helper: true once `limit` ns have passed since `t0`.
@@ -355,50 +359,60 @@ GCC_D int tpl_lock(const KParams &p, uint32_t row, uint32_t tx, bool rd) {
                 : (rd ? tpl_shared<WD>(p, row, tx) : tpl_excl<WD>(p, row, tx));
 }
 
-// First attempts take all locks at once (one ballot decides); retries take
-// them one request at a time in request (= ascending key) order, as the
-// reference does, so that competing transactions cannot keep aborting each
-// other. Both apply the scheme's rule: a conflict means abort (no-wait) or
-// wait-or-die by transaction age (wait-die).
+// First attempts take all locks at once (one ballot decides); after
+// ordered_after failed attempts a retry takes them one request at a time,
+// so that competing transactions cannot keep aborting each other. Both
+// apply the scheme's rule: a conflict means abort (no-wait) or wait-or-die
+// by transaction age (wait-die). Which locks a transaction takes and the
+// rule applied to each never change; only the order of the acquisitions:
+//   * by default a one-at-a-time retry takes every lock but one at once and
+//     then the one whose request failed in the previous attempt: that lock
+//     is contended, and taken last it is held the shortest time (taken in
+//     request order, the reference's order, the hottest key of a Zipf
+//     dataset comes first and is held while 15 more locks are taken one by
+//     one, which made each writer of the hottest row cost ~15 us);
+//   * GCC_F_REQUEST_ORDER, and a starving transaction, keep request (=
+//     ascending key) order;
+//   * a lock plan (p.plan, set by the scheduler from its key-frequency
+//     table) lists the hot requests: the others are taken at once, then the
+//     hot ones one at a time, the hottest last.
 template <int G, bool WD, bool SLOW, class TX>
 GCC_D int attempt_tpl(const KParams &p, const Group<G> &g, const TX &s, uint32_t tx,
                       uint64_t pos, unsigned long long &dg, Clocks &ck, bool ordered) {
     constexpr int K = TX::K;
-    uint32_t held = 0, pending = s.valid;
+    uint32_t held = 0;
     bool fail = false, err = false;
-    uint32_t obst = kNoRow;  // row whose lock request failed
-    bool obst_x = false;     // ... and whether it was an exclusive request
+    uint32_t obst = kNoRow;         // row whose lock request failed
+    bool obst_x = false;            // ... and whether it was an exclusive request
+    uint32_t obst_i = 0xFFFFFFFFu;  // ... and its request index
     uint64_t t0 = gtimer();
     long long cw = clock64();
     bool first = true;
-    if (ordered) {
-        for (uint32_t i = 0; i < s.n && !fail; ++i) {
-            const int owner = (int)(i % G), kk = (int)(i / G);
-            int r = L_OK;
-            if (g.glane == owner) {
-#pragma unroll
-                for (int k = 0; k < K; ++k) {
-                    if (k != kk) continue;
-                    while (true) {
-                        r = tpl_lock<WD, SLOW>(p, s.row[k], tx, (s.isread >> k) & 1u);
-                        if (r != L_WAIT) break;
-                        if (first) { first = false; cw = clock64(); }
-        wait_pause();
-                        if (expired(t0, p.spin_limit_ns) || error_raised(p.ctr)) {
-                            set_error(p.ctr, GCC_ETIMEOUT, W_TPL_WD);
-                            r = L_ERR;
-                            break;
-                        }
-                    }
-                    if (r == L_OK) held |= 1u << k;
-                    else if (r == L_DIE) { obst = s.row[k]; obst_x = !((s.isread >> k) & 1u); }
-                }
-            }
-            r = g.bcast(r, owner);
-            if (r == L_DIE) fail = true;
-            else if (r == L_ERR) { fail = true; err = true; }
+    // planned: this attempt locks the requests outside the plan at once, then
+    // the plan's requests in plan order; late bit k: op glane + k * G is planned
+    bool planned = false;
+    unsigned long long pl = 0;
+    uint32_t late = 0;
+    if constexpr (TX::MAXOPS == kMaxOps) {
+        if (ordered && p.plan != nullptr) {
+            planned = true;
+            pl = __ldg(p.plan + tx);
+        } else if (ordered && !(p.flags & GCC_F_REQUEST_ORDER) && s.obst_op) {
+            // a one-entry plan: the request that failed last time, last
+            planned = true;
+            const unsigned long long i = s.obst_op - 1u;
+            pl = (1ull << i) | (1ull << 16) | (i << 20);
         }
-    } else {
+        if (planned) {
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+                if ((plan_mask(pl) >> (g.glane + k * G)) & 1u) late |= 1u << k;
+        }
+    }
+    uint32_t pending = s.valid & ~late;
+    // every pending request at once; a conflict fails the attempt (no-wait)
+    // or, under wait-die, a younger holder makes the request wait
+    auto lock_at_once = [&]() {
         while (true) {
 #pragma unroll
             for (int k = 0; k < K; ++k) {
@@ -409,6 +423,7 @@ GCC_D int attempt_tpl(const KParams &p, const Group<G> &g, const TX &s, uint32_t
                     fail = true;
                     obst = s.row[k];
                     obst_x = !((s.isread >> k) & 1u);
+                    obst_i = (uint32_t)(g.glane + k * G);
                 }
                 else if (r == L_ERR) err = true;
             }
@@ -416,12 +431,54 @@ GCC_D int attempt_tpl(const KParams &p, const Group<G> &g, const TX &s, uint32_t
             if (ge) { fail = true; err = true; break; }
             if (gf || !gp) { fail = gf; break; }
             if (first) { first = false; cw = clock64(); }
-        wait_pause();
+            wait_pause();
             if (g.any(expired(t0, p.spin_limit_ns) || error_raised(p.ctr))) {
                 if (g.glane == 0) set_error(p.ctr, GCC_ETIMEOUT, W_TPL_WD);
                 fail = true; err = true; break;
             }
         }
+    };
+    if (ordered) {
+        if (planned) lock_at_once();  // the requests outside the plan
+        const uint32_t n_seq = planned ? plan_count(pl) : s.n;
+        for (uint32_t j = 0; j < n_seq && !fail; ++j) {
+            const uint32_t i = planned ? plan_op(pl, j) : j;
+            const int owner = (int)(i % G), kk = (int)(i / G);
+            int r = L_OK;
+            if (g.glane == owner) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    if (k != kk || !((s.valid >> k) & 1u) || ((held >> k) & 1u)) continue;
+                    while (true) {
+                        r = tpl_lock<WD, SLOW>(p, s.row[k], tx, (s.isread >> k) & 1u);
+                        if (r != L_WAIT) break;
+                        if (first) { first = false; cw = clock64(); }
+                        wait_pause();
+                        if (expired(t0, p.spin_limit_ns) || error_raised(p.ctr)) {
+                            set_error(p.ctr, GCC_ETIMEOUT, W_TPL_WD);
+                            r = L_ERR;
+                            break;
+                        }
+                    }
+                    if (r == L_OK) held |= 1u << k;
+                    else if (r == L_DIE) {
+                        obst = s.row[k];
+                        obst_x = !((s.isread >> k) & 1u);
+                        obst_i = i;
+                    }
+                }
+            }
+            r = g.bcast(r, owner);
+            if (r == L_DIE) fail = true;
+            else if (r == L_ERR) { fail = true; err = true; }
+        }
+        // a plan only orders: whatever it did not list is locked now
+        if (planned && !fail) {
+            pending = s.valid & ~held;
+            lock_at_once();
+        }
+    } else {
+        lock_at_once();
     }
     if (!first) ck.wait += clock64() - cw;
     if (fail) {
@@ -429,6 +486,10 @@ GCC_D int attempt_tpl(const KParams &p, const Group<G> &g, const TX &s, uint32_t
         for (int k = 0; k < K; ++k)
             if ((held >> k) & 1u) tpl_unlock<SLOW>(p, s.row[k], (s.isread >> k) & 1u);
         if (err) return kGiveUp;
+        if (!(p.flags & GCC_F_REQUEST_ORDER)) {
+            const uint32_t fi = __reduce_min_sync(g.mask, obst_i);
+            s.obst_op = fi == 0xFFFFFFFFu ? 0u : fi + 1u;
+        }
         // an exclusive request waits for a free word, a shared one for the
         // exclusive holder to leave
         await_row(p, obst, tpl::kExcl, obst_x);
@@ -538,12 +599,28 @@ GCC_D int attempt_to(const KParams &p, const Group<G> &g, const TX &s, uint32_t 
         if (g.glane == 0) set_error(p.ctr, GCC_EOVERFLOW, 0);
         return kGiveUp;
     }
-    uint32_t pending = s.valid, wrote = 0;
+    uint32_t wrote = 0;
     unsigned long long prev[K];
     bool fail = false, err = false;
     uint64_t t0 = gtimer();
     bool first = true;
     long long cw = 0;
+    uint32_t fail_i = 0xFFFFFFFFu;  // request index of this lane's failed op
+    // A one-at-a-time retry visits every request but one at once first and
+    // then the one that failed in the previous attempt, so a contended row
+    // is held uncommitted the shortest time (unless GCC_F_REQUEST_ORDER, or
+    // the transaction is starving: all one at a time in request order, the
+    // reference's order); late bit k: op glane + k * G is that one.
+    uint32_t late = 0, late_i = 0xFFFFFFFFu;
+    if constexpr (TX::MAXOPS == kMaxOps) {
+        if (ordered && !(p.flags & GCC_F_REQUEST_ORDER) && s.obst_op) {
+            late_i = s.obst_op - 1u;
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+                if ((uint32_t)(g.glane + k * G) == late_i) late |= 1u << k;
+        }
+    }
+    uint32_t pending = s.valid & ~late;
     // One request: read (waits while an older writer's version is
     // uncommitted) or write (marks the row uncommitted with this ts).
     auto op = [&](int k) -> int {
@@ -557,37 +634,12 @@ GCC_D int attempt_to(const KParams &p, const Group<G> &g, const TX &s, uint32_t 
             r = to_write<SLOW>(p, s.row[k], ts, prev[k]);
             if (r == O_DONE) wrote |= 1u << k;
         }
+        if (r == O_FAIL) fail_i = i;
         return r;
     };
-    if (ordered) {
-        // Retries visit the requests one at a time in request (= ascending
-        // key) order like the reference, so two writers cannot keep holding
-        // each other's rows uncommitted and aborting each other.
-        for (uint32_t i = 0; i < s.n && !fail; ++i) {
-            const int owner = (int)(i % G), kk = (int)(i / G);
-            int r = O_DONE;
-            if (g.glane == owner) {
-#pragma unroll
-                for (int k = 0; k < K; ++k) {
-                    if (k != kk) continue;
-                    while (true) {
-                        r = op(k);
-                        if (r != O_RETRY) break;
-                        if (first) { first = false; cw = clock64(); }
-        wait_pause();
-                        if (expired(t0, p.spin_limit_ns) || error_raised(p.ctr)) {
-                            set_error(p.ctr, GCC_ETIMEOUT, W_TO_READ);
-                            r = O_ERR;
-                            break;
-                        }
-                    }
-                }
-            }
-            r = g.bcast(r, owner);
-            if (r == O_FAIL) fail = true;
-            else if (r == O_ERR) fail = err = true;
-        }
-    } else {
+    // every pending request at once (reads of rows an older writer holds
+    // uncommitted wait and retry)
+    auto all_at_once = [&]() {
         while (true) {
 #pragma unroll
             for (int k = 0; k < K; ++k) {
@@ -601,12 +653,50 @@ GCC_D int attempt_to(const KParams &p, const Group<G> &g, const TX &s, uint32_t 
             if (ge) { fail = err = true; break; }
             if (gf || !gp) { fail = gf; break; }
             if (first) { first = false; cw = clock64(); }
-        wait_pause();
+            wait_pause();
             if (g.any(expired(t0, p.spin_limit_ns) || error_raised(p.ctr))) {
                 if (g.glane == 0) set_error(p.ctr, GCC_ETIMEOUT, W_TO_READ);
                 fail = err = true; break;
             }
         }
+    };
+    if (ordered) {
+        // Retries visit the requests one at a time, so two writers cannot
+        // keep holding each other's rows uncommitted and aborting each other.
+        const bool split = late_i != 0xFFFFFFFFu;
+        if (split) all_at_once();  // the others
+        const uint32_t n_seq = split ? 1u : s.n;
+        for (uint32_t j = 0; j < n_seq && !fail; ++j) {
+            const uint32_t i = split ? late_i : j;
+            const int owner = (int)(i % G), kk = (int)(i / G);
+            int r = O_DONE;
+            if (g.glane == owner) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    if (k != kk || !((s.valid >> k) & 1u)) continue;
+                    while (true) {
+                        r = op(k);
+                        if (r != O_RETRY) break;
+                        if (first) { first = false; cw = clock64(); }
+                        wait_pause();
+                        if (expired(t0, p.spin_limit_ns) || error_raised(p.ctr)) {
+                            set_error(p.ctr, GCC_ETIMEOUT, W_TO_READ);
+                            r = O_ERR;
+                            break;
+                        }
+                    }
+                }
+            }
+            r = g.bcast(r, owner);
+            if (r == O_FAIL) fail = true;
+            else if (r == O_ERR) fail = err = true;
+        }
+    } else {
+        all_at_once();
+    }
+    if (fail && !err && !(p.flags & GCC_F_REQUEST_ORDER)) {
+        const uint32_t fi = __reduce_min_sync(g.mask, fail_i);
+        s.obst_op = fi == 0xFFFFFFFFu ? 0u : fi + 1u;
     }
     if (!first) ck.wait += clock64() - cw;
     if (fail) {
@@ -1162,10 +1252,13 @@ GCC_D int attempt(const KParams &p, const Group<G> &g, const TX &s, uint32_t tx,
 
 __host__ __device__ constexpr bool is_ordered(int s) { return s == S_GACCO || s == S_GPUTX; }
 
-// Attempts before retries switch to one request at a time in key order.
+// Attempts before retries switch to one request at a time (the caller can
+// move the switch of 2PL / TO with gcc_run_params.ordered_after).
 // Retries take their requests in parallel like the first attempt: Silo and
 // TicToc always, TO and 2PL for their first 15 retries, after which they go
-// one request at a time in key order. The starvation control bounds the
+// one request at a time (starting from the request that failed last time,
+// see attempt_tpl / attempt_to; in key order under GCC_F_REQUEST_ORDER, which
+// is what the measurements below used). The starvation control bounds the
 // cycles that made fully parallel retries livelock. Measured (10,485,760
 // rows, r 0.9) against ordering from the first retry: silo / tictoc +40 %
 // at theta 0.6 and +25-50 % at 0.8-0.99; TO 22.9 -> 57 M tx/s at 0.6 and
@@ -1278,6 +1371,7 @@ __global__ void __launch_bounds__(1024, 1) ycsb_kernel(const __grid_constant__ K
         }
         s.n = (uint32_t)n64;
         s.valid = s.isread = 0;
+        s.obst_op = 0;
         bool miss = false;
         unsigned long long myreads = 0;
 #pragma unroll
@@ -1314,16 +1408,24 @@ __global__ void __launch_bounds__(1024, 1) ycsb_kernel(const __grid_constant__ K
         unsigned long long dg = 0, c_abort = 0;
         long long c_attempt = c_after_idx;
         bool starving = false;
+        // (the caller's ordered_from applies to the schemes that switch, 2PL / TO)
+        const unsigned ord_from = (p.ordered_from && ordered_after(SCH) == 16u)
+                                      ? p.ordered_from - 1u : ordered_after(SCH);
         while (true) {
             dg = 0;
             c_attempt = clock64();
-            st = attempt<SCH, G>(p, g, s, tx, pos, dg, ck, attempts >= ordered_after(SCH));
+            st = attempt<SCH, G>(p, g, s, tx, pos, dg, ck, attempts >= ord_from);
             if (st != kAbort) break;
             ++attempts;
             if (p.starve_limit && attempts == p.starve_limit) {
                 starving = true;
                 if (g.glane == 0) atomicAdd(&p.ctr->starving, 1u);
             }
+            // a starving transaction retries in request order (the
+            // failed-request-last order can keep a timestamp check or a
+            // reader-held row failing for a transaction that already lost
+            // many times; request order is the reference's)
+            if (starving) s.obst_op = 0;
             // A transaction still aborting after 4 x starve_limit attempts
             // retries only while it holds the starvation token: the others
             // at that stage wait between attempts, holding nothing, so the

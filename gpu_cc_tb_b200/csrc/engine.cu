@@ -660,7 +660,7 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
 
     int occ = scheme_occupancy(s, G, block);
     if (occ <= 0) return GCC_EINVAL;  // block too large for this kernel
-    if (rp->max_active < 0 || rp->starve_limit < -1) return GCC_EINVAL;
+    if (rp->max_active < 0 || rp->starve_limit < -1 || rp->ordered_after < 0) return GCC_EINVAL;
     const uint64_t max_grid = std::min<uint64_t>((uint64_t)occ * e->sm_count,
                                                  active_grid(rp->max_active, G, block));
 
@@ -673,6 +673,7 @@ int gcc_run(gcc_engine *e, const gcc_run_params *rp, gcc_result *out) {
     if (rp->backoff_ns < -1 || rp->backoff_ns > 100000) return GCC_EINVAL;
     p.backoff_ns = rp->backoff_ns < 0 ? 0u : (rp->backoff_ns == 0 ? 512u : (uint32_t)rp->backoff_ns);
     p.starve_limit = starve_param(rp->starve_limit);
+    p.ordered_from = rp->ordered_after > 0 ? (uint32_t)rp->ordered_after + 1u : 0u;
     p.scratch = rowcopy ? e->scratch : nullptr;
     p.read_log = want_log ? e->read_log : nullptr;
     p.ver_ts = e->ver_ts;
@@ -1038,6 +1039,7 @@ int gcc_run_batches(gcc_engine *e, const gcc_run_params *rp, const uint32_t *bat
     p.spin_limit_ns = rp->spin_limit_ns ? rp->spin_limit_ns : 4000000000ull;
     p.backoff_ns = rp->backoff_ns < 0 ? 0u : (rp->backoff_ns == 0 ? 512u : (uint32_t)rp->backoff_ns);
     p.starve_limit = starve_param(rp->starve_limit);
+    p.ordered_from = rp->ordered_after > 0 ? (uint32_t)rp->ordered_after + 1u : 0u;
     p.ext_ops = (rp->flags & GCC_F_EXT_OPS) ? 1u : 0u;
     p.ver_ts = e->ver_ts;
     p.ver_prev = e->ver_prev;
@@ -1565,10 +1567,12 @@ struct gcc_sched {
     uint64_t part_cap = 0;
     uint32_t *counts = nullptr;
     float *sums = nullptr;
+    unsigned long long *plan = nullptr;  // 2PL lock plans, by tx id
+    uint64_t plan_cap = 0;
     std::vector<gcc_sched_batch> batches;
     // Policy: the arms of the scheme (0 = plain ordering, then deferral with
-    // in-flight caps 2048 / 1024 / 512 / 256, then for 2PL wait-die at 1024
-    // and 512), an incumbent arm, and the arms compared with it since the
+    // in-flight caps 2048 / 1024 / 512 / 256 / 128, then for 2PL wait-die at
+    // 1024 and 512), an incumbent arm, and the arms compared with it since the
     // last refresh. A refresh happens when the mean prediction of a batch
     // has moved by more than 0.1 since the previous refresh (the contention
     // changed) or after 16 batches.
@@ -1580,7 +1584,7 @@ struct gcc_sched {
     float ref_pred = -1.f;
     ~gcc_sched() {
         if (e) cudaSetDevice(e->dev);
-        void *bufs[] = {order, part_scratch, counts, sums};
+        void *bufs[] = {order, part_scratch, counts, sums, plan};
         for (void *b : bufs)
             if (b) cudaFree(b);
     }
@@ -1591,7 +1595,7 @@ struct gcc_sched {
     void set_arms(int s) {
         arms.clear();
         arms.push_back({0u, 0u, 0u});
-        for (uint32_t c : {2048u, 1024u, 512u, 256u}) arms.push_back({c, 0u, 1u});
+        for (uint32_t c : {2048u, 1024u, 512u, 256u, 128u}) arms.push_back({c, 0u, 1u});
         if (s == S_TPL_NW || s == S_TPL_WD)
             for (uint32_t c : {1024u, 512u}) arms.push_back({c, 1u, 1u});
         inc = 0;
@@ -1615,12 +1619,13 @@ struct gcc_sched {
                 if (!arms[k].wd && (arms[k].defer ? arms[k].cap : 0u) == cap) return k;
             return -1;
         };
-        static const uint32_t kCaps[] = {0u, 2048u, 1024u, 512u, 256u};
+        static const uint32_t kCaps[] = {0u, 2048u, 1024u, 512u, 256u, 128u};
+        constexpr int kNumCaps = 6;
         int r = 0;
         const uint32_t mycap = a.defer ? a.cap : 0u;
-        while (r < 5 && kCaps[r] != mycap) ++r;
+        while (r < kNumCaps && kCaps[r] != mycap) ++r;
         for (int nr : {r + 1, r - 1}) {
-            if (nr < 0 || nr >= 5) continue;
+            if (nr < 0 || nr >= kNumCaps) continue;
             const int k = plain_cap_arm(kCaps[nr]);
             if (k >= 0 && k != inc && !tried[k]) return k;
         }
@@ -1644,6 +1649,7 @@ int gcc_sched_create(gcc_engine *e, const gcc_sched_params *p, gcc_sched **out) 
         p->fixed_arm < 0 || p->min_sched < -1)
         return GCC_EINVAL;
     if (p->minibatch > (1 << 20) || p->probe_rows > (1 << 20)) return GCC_EINVAL;
+    if (p->plan_threshold < -1 || p->plan_after < -1) return GCC_EINVAL;
     if (!(p->lr >= 0.f) || !(p->defer_threshold >= 0.f) || p->defer_threshold >= 1.f)
         return GCC_EINVAL;
     cudaSetDevice(e->dev);
@@ -1657,6 +1663,8 @@ int gcc_sched_create(gcc_engine *e, const gcc_sched_params *p, gcc_sched **out) 
     if (!s->prm.min_sched) s->prm.min_sched = 4096;
     if (s->prm.lr == 0.f) s->prm.lr = 2e-3f;
     if (s->prm.defer_threshold == 0.f) s->prm.defer_threshold = 0.2f;
+    if (!s->prm.plan_threshold) s->prm.plan_threshold = 1024;
+    if (!s->prm.plan_after) s->prm.plan_after = 1;
     cudaError_t ce = s->pred.init(e->dev, e->stream,
                                   (uint64_t)std::max(4096, std::max(s->prm.minibatch, s->prm.probe_rows)),
                                   p->seed);
@@ -1697,6 +1705,28 @@ int gcc_sched_features(gcc_sched *s, uint64_t first, uint64_t n, uint16_t *dst) 
     if (ce == cudaSuccess && n)
         ce = cudaMemcpyAsync(dst, s->pred.feat, n * sched::kFeatStride * 2, cudaMemcpyDeviceToHost,
                              e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    return ce == cudaSuccess ? GCC_OK : s->fail(ce);
+}
+
+int gcc_sched_lock_plans(gcc_sched *s, uint64_t first, uint64_t n, uint64_t *dst) {
+    if (!s || (!dst && n) || n > (1ull << 20)) return GCC_EINVAL;
+    gcc_engine *e = s->e;
+    if (!e->txs || first + n > e->n_rec) return GCC_ESTATE;
+    if (s->prm.plan_threshold <= 0) return GCC_EINVAL;
+    cudaSetDevice(e->dev);
+    cudaError_t ce = cudaSuccess;
+    if (s->plan_cap < e->n_rec) {
+        if (s->plan) cudaFree(s->plan);
+        s->plan = nullptr;
+        s->plan_cap = 0;
+        ce = cudaMalloc(&s->plan, e->n_rec * 8);
+        if (ce == cudaSuccess) s->plan_cap = e->n_rec;
+    }
+    if (ce == cudaSuccess)
+        ce = s->pred.lock_plan(e->txs, first, n, (uint32_t)s->prm.plan_threshold, s->plan);
+    if (ce == cudaSuccess && n)
+        ce = cudaMemcpyAsync(dst, s->plan + first, n * 8, cudaMemcpyDeviceToHost, e->stream);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
     return ce == cudaSuccess ? GCC_OK : s->fail(ce);
 }
@@ -1825,7 +1855,7 @@ struct SchedRun {
     gcc_engine *e = nullptr;
     const gcc_run_params *rp = nullptr;
     int s = 0, G = 0, block = 0, occ_main = 0, occ_wd = 0;
-    bool var = false, learned = false;
+    bool var = false, learned = false, planned = false;
     uint64_t user_grid = 0, batch_index = 0;
     KParams base;
     cudaEvent_t ev0, ev1, evk0, evk1, evt0, evt1, evp1, evq;
@@ -1853,7 +1883,7 @@ int sched_setup(SchedRun &R, gcc_sched *sc, const gcc_run_params *rp, bool var, 
     if (!var && (rp->flags & GCC_F_EXT_OPS)) return GCC_EINVAL;
     if (!ext_ops_allowed(e, s, rp)) return GCC_EINVAL;
     if (rp->backoff_ns < -1 || rp->backoff_ns > 100000) return GCC_EINVAL;
-    if (rp->max_active < 0 || rp->starve_limit < -1) return GCC_EINVAL;
+    if (rp->max_active < 0 || rp->starve_limit < -1 || rp->ordered_after < 0) return GCC_EINVAL;
     if (max_batch == 0 || max_batch > (1ull << 20)) return GCC_EINVAL;
     cudaSetDevice(e->dev);
     R.s = s;
@@ -1868,6 +1898,14 @@ int sched_setup(SchedRun &R, gcc_sched *sc, const gcc_run_params *rp, bool var, 
         sc->order = nullptr;
         if ((ce = cudaMalloc(&sc->order, n * 4))) return sc->fail(ce);
         sc->order_cap = n;
+    }
+    // lock plans: 2PL on 16-request records
+    R.planned = !var && (s == S_TPL_NW || s == S_TPL_WD) && sc->prm.plan_threshold > 0;
+    if (R.planned && sc->plan_cap < n) {
+        if (sc->plan) cudaFree(sc->plan);
+        sc->plan = nullptr;
+        if ((ce = cudaMalloc(&sc->plan, n * 8))) return sc->fail(ce);
+        sc->plan_cap = n;
     }
     const uint64_t pneed = (max_batch + 1023) / 1024 * 3;
     if (sc->part_cap < pneed) {
@@ -1896,6 +1934,7 @@ int sched_setup(SchedRun &R, gcc_sched *sc, const gcc_run_params *rp, bool var, 
     b.spin_limit_ns = rp->spin_limit_ns ? rp->spin_limit_ns : 4000000000ull;
     b.backoff_ns = rp->backoff_ns < 0 ? 0u : (rp->backoff_ns == 0 ? 512u : (uint32_t)rp->backoff_ns);
     b.starve_limit = starve_param(rp->starve_limit);
+    b.ordered_from = rp->ordered_after > 0 ? (uint32_t)rp->ordered_after + 1u : 0u;
     R.user_grid = std::min<uint64_t>((uint64_t)R.occ_main * e->sm_count,
                                      active_grid(rp->max_active, R.G, R.block));
     int rc;
@@ -1917,12 +1956,16 @@ int sched_batch(SchedRun &R, uint64_t bst, uint64_t bn, gcc_sched_batch &rec) {
     cudaStream_t st = e->stream;
     cudaError_t ce;
     auto launch = [&](int sch, uint64_t b0, uint64_t cnt, const uint32_t *order,
-                      uint64_t grid_cap) -> cudaError_t {
+                      uint64_t grid_cap, bool planned = false) -> cudaError_t {
         KParams q = R.base;
         q.batch_st = (uint32_t)b0;
         q.batch_n = (uint32_t)cnt;
         q.order = order;
         q.wait_die = sch == S_TPL_WD ? 1u : 0u;
+        if (planned) {
+            q.plan = sc->plan;
+            q.ordered_from = sc->prm.plan_after < 0 ? 1u : (uint32_t)sc->prm.plan_after + 1u;
+        }
         k_batch_prep<<<1, 32, 0, st>>>(e->ctr, 0);
         cudaError_t c = cudaGetLastError();
         if (c != cudaSuccess) return c;
@@ -1939,17 +1982,18 @@ int sched_batch(SchedRun &R, uint64_t bst, uint64_t bn, gcc_sched_batch &rec) {
     // one part of a batch under an arm: plain ordering (one launch), or the
     // predicted-safe transactions at full concurrency then the deferred ones
     // with the arm's in-flight cap
+    bool pl = false;  // scheduled 2PL batches run with lock plans (set below)
     auto run_part = [&](const SchedArm &a, uint64_t st0, uint64_t cnt, uint32_t n_low) -> cudaError_t {
         if (!cnt) return cudaSuccess;
-        if (!a.defer) return launch(s, st0, cnt, nullptr, R.user_grid);
+        if (!a.defer) return launch(s, st0, cnt, nullptr, R.user_grid, pl);
         cudaError_t c = cudaSuccess;
-        if (n_low) c = launch(s, st0, n_low, sc->order, R.user_grid);
+        if (n_low) c = launch(s, st0, n_low, sc->order, R.user_grid, pl);
         if (c == cudaSuccess && cnt > n_low) {
             const int sch2 = a.wd ? S_TPL_WD : s;
             const int occ2 = a.wd ? R.occ_wd : R.occ_main;
             const uint64_t cap_grid = std::min<uint64_t>((uint64_t)occ2 * e->sm_count,
                                                          active_grid((int32_t)a.cap, G, block));
-            c = launch(sch2, st0 + n_low, cnt - n_low, sc->order, cap_grid);
+            c = launch(sch2, st0 + n_low, cnt - n_low, sc->order, cap_grid, pl);
         }
         return c;
     };
@@ -1976,6 +2020,11 @@ int sched_batch(SchedRun &R, uint64_t bst, uint64_t bn, gcc_sched_batch &rec) {
                    : sc->pred.features(e->txs, bst, bn, sc->pred.feat);
         if (ce == cudaSuccess) ce = sc->pred.forward(sc->pred.feat, bn, sc->pred.p);
         e->kernel_launches += 4;  // features, 2 GEMMs + head
+        if (ce == cudaSuccess && R.planned) {
+            ce = sc->pred.lock_plan(e->txs, bst, bn, (uint32_t)sc->prm.plan_threshold, sc->plan);
+            e->kernel_launches += 1;
+            pl = true;
+        }
         float hsums[4] = {0.f, 0.f, 0.f, 0.f};
         if (ce == cudaSuccess) {
             ce = sched::partition(sc->pred.p, bst, bn, sc->prm.defer_threshold, sc->order + bst,

@@ -175,7 +175,19 @@ struct KParams {
     uint32_t backoff_ns;        // 0: retry at once
     uint32_t starve_limit;      // 0: no starvation control
     uint32_t ext_ops;           // the loaded transactions hold extended ops
+    // 2PL lock plan of each transaction (indexed by tx id, 16-request
+    // records only; null: none). Bits 0-15 mark the requests locked after
+    // the others, one at a time; bits 16-19 count them (<= kPlanMax) and
+    // nibble j at bit 20 + 4j is the request index of the j-th of them.
+    const unsigned long long *plan;
+    uint32_t ordered_from;      // attempts from which 2PL / TO visit one request
+                                // at a time: 0 = the scheme's default, k = k - 1
 };
+
+constexpr int kPlanMax = 11;  // planned requests that fit the nibble list
+GCC_HD uint32_t plan_mask(unsigned long long pl) { return (uint32_t)(pl & 0xFFFFull); }
+GCC_HD uint32_t plan_count(unsigned long long pl) { return (uint32_t)((pl >> 16) & 0xFull); }
+GCC_HD uint32_t plan_op(unsigned long long pl, uint32_t j) { return (uint32_t)((pl >> (20 + 4 * j)) & 0xFull); }
 
 // ---------------------------------------------------------------------------
 // Small device helpers.

@@ -142,6 +142,51 @@ __global__ void k_freq_add(const gcc_ycsb_tx *__restrict__ txs, uint64_t first, 
     atomicAdd(freq + freq_slot((uint32_t)rq.y), 1u);
 }
 
+// Lock plan of each transaction (KParams::plan): half-warp per transaction,
+// lane l holds request l with c = its key's counter in the frequency table.
+// Requests with c >= thr are planned, ordered by (c, key) ascending so the
+// hottest key is locked last; every transaction of the batch compares two
+// keys the same way (one table snapshot), so the plans agree on a global
+// order of the keys they share. At most kPlanMax are planned (the hottest).
+__global__ void k_lock_plan(const gcc_ycsb_tx *__restrict__ txs, uint64_t first, uint64_t n,
+                            const uint32_t *__restrict__ freq, uint32_t thr,
+                            unsigned long long *__restrict__ plan) {
+    const uint64_t t = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
+    const unsigned l = threadIdx.x & 15u;
+    const bool live = t < n;
+    uint32_t c = 0u, key = 0u;
+    bool hot = false;
+    if (live) {
+        const gcc_ycsb_tx *T = txs + first + t;
+        const uint64_t cnt = T->request_cnt;
+        if ((uint64_t)l < cnt) {
+            key = (uint32_t)T->requests[l].key;
+            c = __ldg(freq + freq_slot(key));
+            hot = c >= thr;
+        }
+    }
+    // rank among the hot requests of the transaction by (c, key)
+    unsigned rank = 0u, nhot = 0u;
+    const unsigned seg = threadIdx.x & 16u;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const uint32_t cj = __shfl_sync(0xFFFFFFFFu, c, (int)(seg | (unsigned)j));
+        const uint32_t kj = __shfl_sync(0xFFFFFFFFu, key, (int)(seg | (unsigned)j));
+        const bool hj = __shfl_sync(0xFFFFFFFFu, hot ? 1 : 0, (int)(seg | (unsigned)j)) != 0;
+        nhot += hj ? 1u : 0u;
+        rank += (hj && (cj < c || (cj == c && kj < key))) ? 1u : 0u;
+    }
+    const unsigned keep = nhot < (unsigned)kPlanMax ? nhot : (unsigned)kPlanMax;
+    unsigned long long v = 0ull;
+    if (hot && rank >= nhot - keep) {
+        const unsigned j = rank - (nhot - keep);
+        v = (1ull << l) | ((unsigned long long)l << (20 + 4 * j));
+    }
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) v |= __shfl_xor_sync(0xFFFFFFFFu, v, o, 16);
+    if (live && l == 0) plan[first + t] = v | ((unsigned long long)keep << 16);
+}
+
 // ---------------------------------------------------------------------------
 // Tiled GEMM: C[m][n] (=, or += across K splits) sum_k A(m,k) B(k,n), with
 // A(m,k) = A[m*sam + k*sak] and B(k,n) = B[k*sbk + n*sbn]; operands are
@@ -522,6 +567,14 @@ cudaError_t Predictor::observe(const gcc_ycsb_tx *txs, uint64_t first, uint64_t 
     if (e != cudaSuccess || n == 0) return e;
     const uint64_t threads = n * 16;
     k_freq_add<<<(unsigned)((threads + 255) / 256), 256, 0, stream>>>(txs, first, n, freq);
+    return cudaGetLastError();
+}
+
+cudaError_t Predictor::lock_plan(const gcc_ycsb_tx *txs, uint64_t first, uint64_t n, uint32_t thr,
+                                 unsigned long long *plan) {
+    if (n == 0) return cudaSuccess;
+    const uint64_t threads = n * 16;
+    k_lock_plan<<<(unsigned)((threads + 255) / 256), 256, 0, stream>>>(txs, first, n, freq, thr, plan);
     return cudaGetLastError();
 }
 

@@ -98,6 +98,11 @@ struct Predictor {
     cudaError_t observe_var(const uint32_t *tx_off, const gcc_ycsb_req *reqs, uint64_t first,
                             uint64_t n);
     cudaError_t clear_freq();
+    // 2PL lock plans (KParams::plan) of transactions first .. first + n - 1
+    // into plan[first ..]: requests whose key counter is >= thr are locked
+    // last, the hottest last of all
+    cudaError_t lock_plan(const gcc_ycsb_tx *txs, uint64_t first, uint64_t n, uint32_t thr,
+                          unsigned long long *plan);
     // p[0 .. n) = network(feat rows); activations stay in h1/h2
     cudaError_t forward(const uint16_t *f, uint64_t n, float *p_out);
     // gradient of the mean BCE over n rows into grad (and the loss summed

@@ -75,6 +75,17 @@ extern "C" {
 #define GCC_F_RETRY_IMMEDIATE 8u /* retry an aborted transaction at once
                                instead of first waiting (up to 50 us) until
                                the row that made it abort looks free */
+#define GCC_F_REQUEST_ORDER 256u /* 2PL and TO retries that visit their
+                               requests one at a time do so in request order
+                               (the reference's order, benchmark/ycsb.cu:
+                               60-98). Without it they take every other
+                               request at once and the one that failed in the
+                               previous attempt last, so that contended row is
+                               locked (2PL) or held uncommitted (TO) the
+                               shortest time; a starving transaction (see
+                               starve_limit) still goes in request order.
+                               Either way the same requests under the same
+                               rule; only the order differs. */
 #define GCC_F_EXT_OPS 64u   /* requests with a negative `read` word are
                                extended ops (GCC_OP_*); without this flag
                                every request with read <= 0 is a YCSB write */
@@ -174,6 +185,10 @@ typedef struct gcc_run_params {
                               up to whole CTAs); 0 = as many as the GPU holds.
                               Under heavy contention fewer in flight abort
                               less. With GCC_F_AUTOTUNE the tuner picks it. */
+    int32_t ordered_after; /* 2PL and TO: failed attempts after which a retry
+                              visits its requests one at a time instead of
+                              all at once; 0 = 15 */
+    int32_t reserved;
 } gcc_run_params;
 
 /* Fields 1-15 are the 15 columns of the reference's output line
@@ -450,15 +465,28 @@ typedef struct gcc_sched_params {
                                 transaction is deferred; 0 = 0.2 */
     int32_t fixed_arm;       /* 0: the policy chooses; k > 0: every batch
                                 runs arm k-1 of: plain ordering, deferral
-                                with in-flight cap 2048, 1024, 512, 256, and
-                                for 2PL wait-die deferral at 1024, 512 */
+                                with in-flight cap 2048, 1024, 512, 256, 128,
+                                and for 2PL wait-die deferral at 1024, 512 */
     int32_t min_sched;       /* batches smaller than this run with plain
                                 ordering and skip the predictor (few
                                 transactions are in flight anyway, and the
                                 scheduling pass would add its latency);
                                 0 = 4096, -1 = schedule every batch */
-    int32_t reserved;
+    int32_t plan_threshold;  /* 2PL lock plans of scheduled batches (16-request
+                                records): a request whose key's counter in the
+                                frequency table is at least this is locked
+                                after the others, one at a time, the hottest
+                                last, so the hottest locks are held the
+                                shortest time (counters are halved after
+                                every batch and count every request, so a
+                                key read or written k times per batch
+                                settles near 2k); 0 = 1024, -1 = no plans */
     uint64_t seed;           /* initial weights (He-uniform from this seed) */
+    int32_t plan_after;      /* attempts after which a planned transaction
+                                locks as planned (before that, all at once);
+                                0 = 1 (from its first retry), -1 = from its
+                                first attempt */
+    int32_t reserved;
 } gcc_sched_params;
 
 typedef struct gcc_sched_batch {
@@ -503,6 +531,14 @@ int gcc_sched_batches(gcc_sched *s, gcc_sched_batch *dst, uint64_t n);
 /* Features of loaded records first .. first+n-1 against the current
  * frequency table: n rows of GCC_SCHED_FEAT_STRIDE u16 (host). */
 int gcc_sched_features(gcc_sched *s, uint64_t first, uint64_t n, uint16_t *dst);
+/* 2PL lock plans of loaded records first .. first+n-1 against the current
+ * frequency table and the scheduler's plan_threshold, as a scheduled batch
+ * computes them (host, one u64 per record): bits 0-15 mark the requests
+ * locked last, bits 16-19 count them (at most 11, the hottest), and nibble j
+ * at bit 20 + 4j is the j-th of them in locking order (the request whose
+ * key has the larger counter later; equal counters by ascending key).
+ * GCC_EINVAL when plans are off (plan_threshold -1). */
+int gcc_sched_lock_plans(gcc_sched *s, uint64_t first, uint64_t n, uint64_t *dst);
 /* Count records first .. first+n-1 into the frequency table (after halving
  * it), as a run does after each batch; clear = 1 zeroes it first. */
 int gcc_sched_observe(gcc_sched *s, uint64_t first, uint64_t n, int32_t clear);

@@ -16,7 +16,10 @@ the engine's predictor implements:
     sigmoid output, with weights rounded to BF16 (round to nearest even);
   * the mean binary cross-entropy against 0/1 labels and its gradient with
     respect to every parameter (flat layout W1[66][128], b1, W2[128][128],
-    b2, w3[128], b3).
+    b2, w3[128], b3);
+  * the 2PL lock plan of a transaction: which requests are locked after the
+    others (key counter >= a threshold) and in which order (the hottest
+    last).
 The predictor has no counterpart in the reference (gCCTB runs transactions
 in index order); these definitions are the checker for the GPU kernels, and
 the gradient itself is pinned by finite differences in tests/.
@@ -131,6 +134,30 @@ def _var_keys(tx_off, reqs, lo, hi):
     cnt = np.diff(tx_off[lo:hi + 1]).astype(np.int64)
     tx = np.repeat(np.arange(hi - lo), cnt)
     return tx, reqs["key"][a:b].astype(np.uint64), reqs["read"][a:b]
+
+
+PLAN_MAX = 11
+
+
+def lock_plans(txs, freq: np.ndarray, thr: int) -> np.ndarray:
+    """2PL lock plan of each record (the scheduler's k_lock_plan): requests
+    whose key counter c >= thr, ordered by (c, key) ascending; at most
+    PLAN_MAX of them, the last ones of that order. u64: bits 0-15 the planned
+    requests, 16-19 their count, nibble j at bit 20 + 4j the j-th request
+    index. Pure-Python loop over records (small cases)."""
+    keys, _, mask = _keys(txs)
+    c = freq[freq_slots(keys)].astype(np.int64)
+    out = np.zeros(len(txs), dtype=np.uint64)
+    for t in range(len(txs)):
+        hot = [(int(c[t, i]), int(keys[t, i]), i) for i in range(16)
+               if mask[t, i] and c[t, i] >= thr]
+        hot.sort()
+        hot = hot[max(0, len(hot) - PLAN_MAX):]
+        v = len(hot) << 16
+        for j, (_, _, i) in enumerate(hot):
+            v |= (1 << i) | (i << (20 + 4 * j))
+        out[t] = v
+    return out
 
 
 def observe_var(freq: np.ndarray, tx_off, reqs, lo, hi) -> np.ndarray:

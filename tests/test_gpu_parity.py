@@ -29,9 +29,9 @@ def expected_order(oracle, scheme, eng, txs, rows):
 
 
 def run_and_check(oracle, eng, init, txs, scheme, wd, bs, batch, write_mode, layout,
-                  write_seed=99, read_log=False, **kw):
+                  write_seed=99, read_log=False, extra_flags=0, **kw):
     eng.upload_table(init)
-    flags = g.F_COMMIT_LOG | (g.F_READ_LOG if read_log else 0)
+    flags = g.F_COMMIT_LOG | (g.F_READ_LOG if read_log else 0) | extra_flags
     res = eng.run(scheme, warp_density=wd, block_size=bs, batch_size=batch, flags=flags,
                   write_mode=write_mode, write_seed=write_seed, spin_limit_ns=SPIN_NS, **kw)
     assert res["committed"] == len(txs)
@@ -124,6 +124,25 @@ def test_starvation_control_and_in_flight_cap(oracle, scheme):
                       starve_limit=2)
         run_and_check(oracle, eng, init, txs, scheme, 3, 8, 1024, g.WRITE_FIELD, layout,
                       max_active=40)
+
+
+@pytest.mark.parametrize("scheme", ["tpl_nw", "tpl_wd", "slow_tpl_nw", "slow_tpl_wd", "to",
+                                    "slow_to"])
+@pytest.mark.parametrize("order_flag,ordered_after", [(0, 1), (0, 3), (g.F_REQUEST_ORDER, 1),
+                                                      (g.F_REQUEST_ORDER, 0)])
+def test_retry_orders(oracle, scheme, order_flag, ordered_after):
+    # 2PL / TO retries that visit their requests one at a time (from the
+    # first retry, or after a few), with the failed request last (default)
+    # or in request order (the reference's order): only the order of the
+    # accesses changes, so every run replays bit-exactly
+    rows, layout = 64, g.LAYOUT_U64X11
+    txs = g.gen_ycsb(rows, 2048, 0.99, 0.5, seed=17, dedup=g.DEDUP_RESAMPLE, key_base=0)
+    init = oracle.fill_table(rows, layout, 9)
+    with g.Engine(rows, layout=layout, index=g.INDEX_DIRECT, fill_seed=9, max_batch=1024) as eng:
+        eng.load_txs(txs)
+        res = run_and_check(oracle, eng, init, txs, scheme, 5, 8, 1024, g.WRITE_FIELD, layout,
+                            ordered_after=ordered_after, extra_flags=order_flag)
+        assert res["aborts"] > 0
 
 
 @pytest.mark.parametrize("scheme", ["tpl_nw", "tictoc", "gacco", "mvcc"])

@@ -67,6 +67,27 @@ def test_forward_and_gradient_match_oracle(eng_small):
             assert not bad.any(), (np.nonzero(bad)[0][:8], np.max(np.abs(grad - gref)), tol)
 
 
+@pytest.mark.parametrize("thr", [1, 4, 64])
+def test_lock_plans_bit_exact(eng_small, thr):
+    # the scheduler's 2PL lock plans against the oracle's, on a frequency
+    # table built from three batches (threshold 1 plans more than 11 requests
+    # of many records, so the cut to the hottest 11 is covered too)
+    eng, txs = eng_small
+    with g.Scheduler(eng, plan_threshold=thr) as sc:
+        freq = np.zeros(1 << P.FREQ_BITS, dtype=np.uint32)
+        sc.observe(0, 0, clear=True)
+        for first in (0, 2000, 4000):
+            sc.observe(first, 2000)
+            freq = P.observe(freq, txs[first:first + 2000])
+        got = sc.lock_plans(0, len(txs))
+        want = P.lock_plans(txs, freq, thr)
+        counts = (want >> np.uint64(16)) & np.uint64(15)
+        assert counts.max() >= 2
+        if thr == 1:
+            assert (counts == 11).any()
+        assert np.array_equal(got, want)
+
+
 def test_training_lowers_loss(eng_small):
     eng, txs = eng_small
     with g.Scheduler(eng, seed=5, minibatch=1024, lr=3e-3) as sc:
@@ -102,20 +123,25 @@ def _write_count_network():
     return w
 
 
-@pytest.mark.parametrize("scheme,arm", [("tpl_nw", 0), ("tpl_nw", 4), ("tpl_wd", 3),
-                                        ("tpl_nw", 7), ("silo", 0), ("silo", 3), ("tictoc", 0),
-                                        ("tictoc", 5)])
-def test_scheduled_runs_are_serializable(oracle, scheme, arm):
-    # arm 0: the policy (probes, in-batch comparisons); arm k > 0: every
-    # batch defers the predicted-risky transactions (more than 8 writes)
-    # into a capped sub-batch of arm k - 1
+@pytest.mark.parametrize("scheme,arm,plan", [
+    ("tpl_nw", 0, 0), ("tpl_nw", 4, 0), ("tpl_wd", 3, 0), ("tpl_nw", 7, 0), ("tpl_nw", 6, 0),
+    ("silo", 0, 0), ("silo", 3, 0), ("tictoc", 0, 0), ("tictoc", 5, 0),
+    ("tpl_nw", 1, 8), ("tpl_wd", 2, 8), ("tpl_nw", 0, -1), ("tpl_nw", 8, 4)])
+def test_scheduled_runs_are_serializable(oracle, scheme, arm, plan):
+    # arm 0: the policy (probes, in-batch comparisons); arm 1: plain
+    # ordering; arm k > 1: every batch defers the predicted-risky
+    # transactions (more than 8 writes) into a capped sub-batch of arm k - 1.
+    # 2PL runs lock by the scheduler's lock plans (plan: 0 = default
+    # threshold, k > 0 = threshold k, which plans most requests of this
+    # table; -1 = no plans)
     rows = 20_000
     txs = g.gen_ycsb(rows, 24_576, 0.95, 0.4, seed=41, dedup=g.DEDUP_RESAMPLE, key_base=0)
     init = oracle.fill_table(rows, g.LAYOUT_U64X11, 8)
     with g.Engine(rows, layout=g.LAYOUT_U64X11, index=g.INDEX_HASH, fill_seed=8,
                   max_batch=4096) as eng, \
             g.Scheduler(eng, explore_every=3, probe_rows=512, train_steps=4 if arm == 0 else -1,
-                        minibatch=512, fixed_arm=arm, defer_threshold=0.5) as sc:
+                        minibatch=512, fixed_arm=arm, defer_threshold=0.5,
+                        plan_threshold=plan, plan_after=-1 if plan > 4 else 0) as sc:
         eng.load_txs(txs)
         if arm:
             sc.set_weights(_write_count_network())
@@ -130,7 +156,9 @@ def test_scheduled_runs_are_serializable(oracle, scheme, arm):
             explored += sum(1 for b in sc.batches() if b["explored"])
         recs = sc.batches()
         assert all(b["kind"] == 1 and b["committed"] > 0 for b in recs)
-        if arm:
+        if arm == 1:
+            assert sum(b["deferred"] for b in recs) == 0  # plain ordering
+        elif arm:
             feat = sc.features(0, len(txs))
             risky = int((feat[:, 64] > 8).sum())
             assert 0 < sum(b["deferred"] for b in recs) <= risky

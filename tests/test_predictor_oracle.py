@@ -70,3 +70,40 @@ def test_features_direct_count():
         heat = sum((int(freq[P.freq_slots(np.array([k]))[0]]) + 1).bit_length() - 1 for k in keys)
         assert f[t, 65] == heat
         assert not f[t, 66:].any()
+
+
+def test_lock_plan_known_answer():
+    # one record: keys 3, 9, 20, 40, 50 (request order); counters chosen so
+    # that keys 9 and 40 tie, key 50 is the hottest and key 3 is cold
+    txs = np.zeros(1, dtype=g.TX_DTYPE)
+    keys = [3, 9, 20, 40, 50]
+    txs[0]["request_cnt"] = len(keys)
+    for i, k in enumerate(keys):
+        txs[0]["requests"][i] = (1 if i % 2 else 0, k)
+    freq = np.zeros(1 << P.FREQ_BITS, dtype=np.uint32)
+    cnt = {3: 5, 9: 300, 20: 1000, 40: 300, 50: 7000}
+    slots = P.freq_slots(np.array(keys, dtype=np.uint64))
+    assert len(set(slots.tolist())) == len(keys)
+    for k, sl in zip(keys, slots):
+        freq[sl] = cnt[k]
+    plan = int(P.lock_plans(txs, freq, 100)[0])
+    # planned: requests 1 (key 9), 3 (key 40), 2 (key 20), 4 (key 50), in
+    # that order: (300, 9) < (300, 40) < (1000, 20) < (7000, 50)
+    assert plan & 0xFFFF == 0b11110
+    assert (plan >> 16) & 0xF == 4
+    assert [(plan >> (20 + 4 * j)) & 0xF for j in range(4)] == [1, 3, 2, 4]
+    # a threshold above every counter plans nothing
+    assert int(P.lock_plans(txs, freq, 10_000)[0]) == 0
+    # more than 11 hot requests: only the 11 hottest are planned
+    txs2 = np.zeros(1, dtype=g.TX_DTYPE)
+    txs2[0]["request_cnt"] = 16
+    keys2 = np.arange(100, 116, dtype=np.uint64)
+    for i in range(16):
+        txs2[0]["requests"][i] = (1, int(keys2[i]))
+    freq2 = np.zeros(1 << P.FREQ_BITS, dtype=np.uint32)
+    for i, sl in enumerate(P.freq_slots(keys2)):
+        freq2[sl] = max(freq2[sl], 1000 + i)
+    plan2 = int(P.lock_plans(txs2, freq2, 1)[0])
+    assert (plan2 >> 16) & 0xF == 11
+    order = [(plan2 >> (20 + 4 * j)) & 0xF for j in range(11)]
+    assert order == sorted(order) and order[-1] == 15
