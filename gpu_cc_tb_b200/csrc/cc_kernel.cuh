@@ -371,8 +371,9 @@ GCC_D int tpl_lock(const KParams &p, uint32_t row, uint32_t tx, bool rd) {
 //     request order, the reference's order, the hottest key of a Zipf
 //     dataset comes first and is held while 15 more locks are taken one by
 //     one, which made each writer of the hottest row cost ~15 us);
-//   * GCC_F_REQUEST_ORDER, and a starving transaction, keep request (=
-//     ascending key) order;
+//   * GCC_F_REQUEST_ORDER and the latch variants keep request (= ascending
+//     key) order (a latch variant's retries taking 15 latches at once kept
+//     a starving transaction of a small hot table from ever committing);
 //   * a lock plan (p.plan, set by the scheduler from its key-frequency
 //     table) lists the hot requests: the others are taken at once, then the
 //     hot ones one at a time, the hottest last.
@@ -397,7 +398,7 @@ GCC_D int attempt_tpl(const KParams &p, const Group<G> &g, const TX &s, uint32_t
         if (ordered && p.plan != nullptr) {
             planned = true;
             pl = __ldg(p.plan + tx);
-        } else if (ordered && !(p.flags & GCC_F_REQUEST_ORDER) && s.obst_op) {
+        } else if (!SLOW && ordered && !(p.flags & GCC_F_REQUEST_ORDER) && s.obst_op) {
             // a one-entry plan: the request that failed last time, last
             planned = true;
             const unsigned long long i = s.obst_op - 1u;
@@ -486,7 +487,7 @@ GCC_D int attempt_tpl(const KParams &p, const Group<G> &g, const TX &s, uint32_t
         for (int k = 0; k < K; ++k)
             if ((held >> k) & 1u) tpl_unlock<SLOW>(p, s.row[k], (s.isread >> k) & 1u);
         if (err) return kGiveUp;
-        if (!(p.flags & GCC_F_REQUEST_ORDER)) {
+        if (!SLOW && !(p.flags & GCC_F_REQUEST_ORDER)) {
             const uint32_t fi = __reduce_min_sync(g.mask, obst_i);
             s.obst_op = fi == 0xFFFFFFFFu ? 0u : fi + 1u;
         }
@@ -608,12 +609,15 @@ GCC_D int attempt_to(const KParams &p, const Group<G> &g, const TX &s, uint32_t 
     uint32_t fail_i = 0xFFFFFFFFu;  // request index of this lane's failed op
     // A one-at-a-time retry visits every request but one at once first and
     // then the one that failed in the previous attempt, so a contended row
-    // is held uncommitted the shortest time (unless GCC_F_REQUEST_ORDER, or
-    // the transaction is starving: all one at a time in request order, the
-    // reference's order); late bit k: op glane + k * G is that one.
+    // is held uncommitted the shortest time. Request order (the reference's)
+    // instead under GCC_F_REQUEST_ORDER, in the latch variant, and for a
+    // starving transaction: TO's conflicts are timestamp checks, and a
+    // starving transaction that reached its contended row last kept meeting
+    // younger readers there (one did not commit within the wait bound at
+    // theta 0.8). late bit k: op glane + k * G is that one.
     uint32_t late = 0, late_i = 0xFFFFFFFFu;
     if constexpr (TX::MAXOPS == kMaxOps) {
-        if (ordered && !(p.flags & GCC_F_REQUEST_ORDER) && s.obst_op) {
+        if (!SLOW && ordered && !(p.flags & GCC_F_REQUEST_ORDER) && s.obst_op) {
             late_i = s.obst_op - 1u;
 #pragma unroll
             for (int k = 0; k < K; ++k)
@@ -694,7 +698,7 @@ GCC_D int attempt_to(const KParams &p, const Group<G> &g, const TX &s, uint32_t 
     } else {
         all_at_once();
     }
-    if (fail && !err && !(p.flags & GCC_F_REQUEST_ORDER)) {
+    if (!SLOW && fail && !err && !(p.flags & GCC_F_REQUEST_ORDER)) {
         const uint32_t fi = __reduce_min_sync(g.mask, fail_i);
         s.obst_op = fi == 0xFFFFFFFFu ? 0u : fi + 1u;
     }
@@ -1421,11 +1425,12 @@ __global__ void __launch_bounds__(1024, 1) ycsb_kernel(const __grid_constant__ K
                 starving = true;
                 if (g.glane == 0) atomicAdd(&p.ctr->starving, 1u);
             }
-            // a starving transaction retries in request order (the
-            // failed-request-last order can keep a timestamp check or a
-            // reader-held row failing for a transaction that already lost
-            // many times; request order is the reference's)
-            if (starving) s.obst_op = 0;
+            // a starving TO transaction retries in request order (see
+            // attempt_to); starving 2PL ones keep the failed lock last, which
+            // is what lets the hot rows' writers through
+            if constexpr (SCH == S_TO) {
+                if (starving) s.obst_op = 0;
+            }
             // A transaction still aborting after 4 x starve_limit attempts
             // retries only while it holds the starvation token: the others
             // at that stage wait between attempts, holding nothing, so the

@@ -75,15 +75,16 @@ extern "C" {
 #define GCC_F_RETRY_IMMEDIATE 8u /* retry an aborted transaction at once
                                instead of first waiting (up to 50 us) until
                                the row that made it abort looks free */
-#define GCC_F_REQUEST_ORDER 256u /* 2PL and TO retries that visit their
-                               requests one at a time do so in request order
-                               (the reference's order, benchmark/ycsb.cu:
-                               60-98). Without it they take every other
-                               request at once and the one that failed in the
-                               previous attempt last, so that contended row is
-                               locked (2PL) or held uncommitted (TO) the
-                               shortest time; a starving transaction (see
-                               starve_limit) still goes in request order.
+#define GCC_F_REQUEST_ORDER 256u /* tpl_nw, tpl_wd and to: retries that
+                               visit their requests one at a time do so in
+                               request order (the reference's order,
+                               benchmark/ycsb.cu:60-98). Without it they take
+                               every other request at once and the one that
+                               failed in the previous attempt last, so that
+                               contended row is locked (2PL) or held
+                               uncommitted (TO) the shortest time; a starving
+                               TO transaction (see starve_limit) and the
+                               latch variants always go in request order.
                                Either way the same requests under the same
                                rule; only the order differs. */
 #define GCC_F_EXT_OPS 64u   /* requests with a negative `read` word are
