@@ -187,6 +187,38 @@ def test_trained_network_beats_plain_ordering(oracle):
         assert gain > 1.3
 
 
+def test_lock_plans_beat_the_best_capped_plain_kernel():
+    # theta 0.99 on the benchmark's table (10,485,760 rows), 8 batches of
+    # 65,536: the learned scheduler with lock plans against (a) the plain
+    # kernel at its best in-flight cap of {128, 256, 512} and (b) the same
+    # scheduler without lock plans. Each plain / scheduled configuration
+    # runs twice and keeps its second run (the scheduler's first run trains
+    # the network and fills the frequency table).
+    rows, nb, bsz = 10_485_760, 8, 65_536
+    txs = g.gen_ycsb(rows, nb * bsz, 0.99, 0.9, seed=20240521, dedup=g.DEDUP_RESAMPLE,
+                     key_base=0)
+    with g.Engine(rows, layout=g.LAYOUT_U64X11, index=g.INDEX_HASH, fill_seed=1,
+                  max_batch=bsz) as eng:
+        eng.load_txs(txs)
+        kw = dict(warp_density=5, block_size=32, batch_size=bsz, write_seed=1,
+                  spin_limit_ns=SPIN)
+        best = 0.0
+        for cap in (128, 256, 512):
+            eng.run("tpl_nw", max_active=cap, **kw)
+            best = max(best, eng.run("tpl_nw", max_active=cap, **kw)["tx_per_s"])
+        rate = {}
+        for name, thr in (("plans", 0), ("no_plans", -1)):
+            with g.Scheduler(eng, mode=g.SCHED_LEARNED, seed=7, plan_threshold=thr) as sc:
+                sc.run("tpl_nw", **kw)
+                r = sc.run("tpl_nw", **kw)
+                assert r["committed"] == len(txs)
+                rate[name] = r["tx_per_s"]
+        print(f"plain best cap {best:.0f} tx/s, learned with plans {rate['plans']:.0f}, "
+              f"without {rate['no_plans']:.0f}")
+        assert rate["plans"] > 1.3 * best
+        assert rate["plans"] > 1.3 * rate["no_plans"]
+
+
 def _auc(p, y):
     """ROC AUC of scores p for 0/1 labels y (rank statistic, ties halved)."""
     y = y.astype(bool)
