@@ -94,6 +94,10 @@ def parse():
                          "learned: 256 drifting-contention batches, learned scheduling")
     ap.add_argument("--sweep-txs", type=int, default=262_144,
                     help="transactions per point of the sweep workload's scheme grid")
+    ap.add_argument("--sweep-grid", type=int, default=1,
+                    help="sweep workload: 0 skips the scheme x theta x read-ratio grid")
+    ap.add_argument("--ref-points", default="ro,mc,hc,t9",
+                    help="sweep workload: the reference's dataset points to run")
     ap.add_argument("--batches", type=int, default=None,
                     help="batches of the batched (64) / learned (256) workloads")
     a = ap.parse_args()
@@ -841,7 +845,7 @@ def run_sweep(a):
 
     with g.Engine(a.rows, layout=g.LAYOUT_U64X11, index=g.INDEX_HASH, fill_seed=141919810,
                   device=local, max_batch=a.batch) as eng:
-        for theta in (0.1, 0.6, 0.8, 0.99):
+        for theta in ((0.1, 0.6, 0.8, 0.99) if a.sweep_grid else ()):
             for r in (1.0, 0.9, 0.5):
                 txs = g.gen_ycsb(a.rows, a.sweep_txs, theta, r, seed=141919810,
                                  dedup=g.DEDUP_RESAMPLE, key_base=0)
@@ -859,6 +863,8 @@ def run_sweep(a):
     ref_points = {}
     from oracle import ref_gpu
     for name, theta, r in (("ro", 0.0, 1.0), ("mc", 0.6, 0.9), ("hc", 0.8, 0.5), ("t9", 0.9, 0.9)):
+        if name not in a.ref_points.split(","):
+            continue
         etx = g.gen_ycsb(a.rows, a.txs, theta, r, seed=141919810, dedup=g.DEDUP_DROP, key_base=1)
         rp = {"engine": {}, "reference": {}}
         with g.Engine(a.rows, layout=g.LAYOUT_REF104, index=g.INDEX_SORTED, fill_seed=0,
