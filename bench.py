@@ -301,8 +301,8 @@ CAPS = (128, 256, 512, 1024, 2048)
 
 
 def learned_vs_plain(g, eng, a, sch, n_batches=16, theta=0.99):
-    """BASELINE's headline comparison on the benchmark's table: n_batches
-    batches of 65,536 transactions at Zipf theta 0.99 (read ratio 0.9),
+    """The headline comparison, learned scheduling against the plain kernels,
+    on the benchmark's table: n_batches batches of 65,536 transactions at Zipf theta 0.99 (read ratio 0.9),
     committed tx/s of
       plain        the plain kernel, one launch per batch, every transaction
                    of the batch in flight the GPU holds;
@@ -799,8 +799,7 @@ def run_serving(a):
 
 
 def run_sweep(a):
-    """The plain-YCSB scheme sweep on one B200 (BASELINE's second
-    configuration): every scheme x theta {0.1, 0.6, 0.8, 0.99} x read ratio
+    """The plain-YCSB scheme sweep on one B200: every scheme x theta {0.1, 0.6, 0.8, 0.99} x read ratio
     {1.0, 0.9, 0.5} at warp_density 5 / block_size 32, and the warp_density
     0-5 x block_size {1, 8, 16, 32} grid at theta 0.6 and 0.99 (tpl_nw and
     silo), on 10,485,760 rows with --txs transactions of 16 requests in
